@@ -1,0 +1,367 @@
+"""Throughput benchmark of the fused lattice-Boltzmann step (one JSON line on stdout).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl b200|reference]
+
+Default workload: D2Q9 BGK, tau = 0.6, 4096 x 4096 fully periodic, fp32 storage (f - w,
+shifted arithmetic), pull two-buffer; rho = 1 + 0.01 N(0,1), u = 8 seeded Fourier modes with
+max|u| = 0.05. One benchmark step = 1000 lattice time steps of the whole lattice. The state
+(2 x 604 MB) is larger than L2, so no flush is needed between steps.
+
+* ``value``    MLUPS with the state resident in HBM, CUDA events on the launching stream,
+               max over ranks (replicas: every rank advances its own lattice, no collective
+               on the data path).
+* ``e2e``      the same through the solver API with host buffers: every step copies the
+               stored state host -> device from pinned memory, advances 1000 steps and copies
+               the state back.
+* ``roofline`` algorithmic bytes (2 q s per node and launch) / average launch time, against
+               the measured HBM copy bandwidth.
+* ``cpu_baseline``  the float64 NumPy oracle (a port of pylbm's own CPU path) on a bounded
+               sample of the same workload, one host core.
+
+``--impl reference`` times that CPU implementation instead, on all host cores (one process
+per core, each advancing its own 4096-wide periodic band of the workload).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+# name -> (lattice, n, collision, tau, variant)
+WORKLOADS = {
+    "d2q9-bgk-ab-f32": ("D2Q9", 4096, "bgk", 0.6, "fused"),
+    "d2q9-trt-ab-f32": ("D2Q9", 4096, "trt", 0.6, "fused"),
+    "d2q9-bgk-aa-f32": ("D2Q9", 4096, "bgk", 0.6, "fused-aa"),
+    "d2q9-trt-aa-f32": ("D2Q9", 4096, "trt", 0.6, "fused-aa"),
+    "d2q9-bgk-ab-f16": ("D2Q9", 4096, "bgk", 0.6, "fused-fp16"),
+    "d2q9-bgk-aa-f16": ("D2Q9", 4096, "bgk", 0.6, "fused-aa-fp16"),
+    "d2q9-bgk-ab-plain": ("D2Q9", 4096, "bgk", 0.6, "fused-plain"),
+    "d3q19-trt-ab-f32": ("D3Q19", 256, "trt", 0.55, "fused"),
+    "d3q19-trt-ab-f16": ("D3Q19", 256, "trt", 0.55, "fused-fp16"),
+    "d3q19-trt-ab-bf16": ("D3Q19", 256, "trt", 0.55, "fused-bf16"),
+    "d3q19-trt-aa-f32": ("D3Q19", 256, "trt", 0.55, "fused-aa"),
+}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a) -> None:  # noqa: ANN002
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_from_profiles(kernel_tag: str) -> float | None:
+    """Per-launch DRAM bytes recorded from an ncu capture in profiles/traffic.json."""
+    p = ROOT / "profiles" / "traffic.json"
+    try:
+        return float(json.loads(p.read_text())[kernel_tag]["bytes_per_launch"])
+    except Exception:
+        return None
+
+
+def make_problem(name: str):
+    from pylbm_b200.problem import Problem
+
+    lat, n, coll, tau, _ = WORKLOADS[name]
+    if lat == "D2Q9":
+        return Problem((n, n), tau=tau, collision=coll, periodic=(True, True))
+    return Problem((n, n, n), tau=tau, collision=coll, periodic=(True, True, True))
+
+
+def initial_state(name: str, seed: int) -> np.ndarray:
+    from pylbm_b200 import workloads as W
+
+    lat, n, *_ = WORKLOADS[name]
+    if lat == "D2Q9":
+        return W.fourier_populations(n, seed)
+    return W.taylor_green_3d_populations(n)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region (read-only)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int) -> None:
+        self.gpu = gpu
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self) -> ClockSampler:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.tmp, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc) -> None:  # noqa: ANN002
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.tmp.flush()
+        rows = []
+        for line in Path(self.tmp.name).read_text().splitlines():
+            parts = [v.strip() for v in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- CPU legs
+def _oracle_band_worker(args: tuple) -> float:
+    """Time ``steps`` oracle steps on one periodic 4096-wide band (runs in a spawned process)."""
+    name, rows, steps, warmup, seed, barrier = args
+    sys.path.insert(0, str(ROOT))
+    from oracle import lbm_oracle as O
+    from pylbm_b200 import workloads as W
+    from pylbm_b200.lattice import D2Q9, D3Q19, equilibrium
+
+    lat, n, coll, tau, _ = WORKLOADS[name]
+    if lat == "D2Q9":
+        rho, u = W.fourier_state(n, seed)
+        f = equilibrium(D2Q9, rho[:rows], u[:, :rows])
+        case = O.Case((n, rows), tau, coll, (True, True))
+    else:
+        rho, u = W.taylor_green_3d(n)
+        f = equilibrium(D3Q19, rho[:rows], u[:, :rows])
+        case = O.Case((n, n, rows), tau, coll, (True, True, True))
+    for _ in range(warmup):
+        f = O.step(f, case)
+    if barrier is not None:
+        barrier.wait()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        f = O.step(f, case)
+    return time.perf_counter() - t0
+
+
+def band_nodes(name: str, rows: int) -> int:
+    lat, n, *_ = WORKLOADS[name]
+    return n * rows if lat == "D2Q9" else n * n * rows
+
+
+def cpu_baseline(name: str) -> dict:
+    """The oracle on one core, a bounded sample of the workload (about 10 s)."""
+    lat = WORKLOADS[name][0]
+    rows, steps = (512, 3) if lat == "D2Q9" else (8, 3)
+    dt = _oracle_band_worker((name, rows, steps, 1, 0, None))
+    mlups = band_nodes(name, rows) * steps / dt / 1e6
+    return {"value": mlups, "unit": "MLUPS", "cores": 1, "kind": "port",
+            "sample": f"float64 NumPy oracle, {steps} steps of a periodic band of "
+                      f"{band_nodes(name, rows)} nodes of the same workload"}
+
+
+def run_reference(a: argparse.Namespace) -> None:
+    """--impl reference: the CPU implementation on all host cores."""
+    import multiprocessing as mp
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    name = a.workload
+    lat = WORKLOADS[name][0]
+    cores = min(os.cpu_count() or 1, a.cpu_procs)
+    rows = 64 if lat == "D2Q9" else 2
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    barrier = mgr.Barrier(cores)
+    with ctx.Pool(cores) as pool:
+        times = pool.map(_oracle_band_worker,
+                         [(name, rows, a.steps, a.warmup, 0, barrier)] * cores)
+    dt = max(times)
+    total = cores * band_nodes(name, rows) * a.steps
+    mlups = total / dt / 1e6
+    sample = (f"float64 NumPy oracle, {cores} processes x {a.steps} steps of a periodic band "
+              f"of {band_nodes(name, rows)} nodes each")
+    out = {"impl": "reference", "metric": "MLUPS", "value": mlups, "unit": "MLUPS",
+           "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": 1e3 * dt / a.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": config_of(name, a),
+           "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": cores, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def config_of(name: str, a: argparse.Namespace) -> dict:
+    lat, n, coll, tau, variant = WORKLOADS[name]
+    shape = [n, n] if lat == "D2Q9" else [n, n, n]
+    return {"workload": name, "lattice": lat, "shape": shape, "collision": coll, "tau": tau,
+            "variant": variant, "periodic": True, "lbm_steps_per_step": a.lbm_steps,
+            "init": ("rho=1+0.01N(0,1), u=8 seeded Fourier modes, max|u|=0.05"
+                     if lat == "D2Q9" else "Taylor-Green vortex u0=0.05, rho=1"),
+            "l2": "state larger than L2 (no flush needed)", "parallelism": f"replicas x{a.gpus}"}
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def run_b200(a: argparse.Namespace) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from pylbm_b200.backend import VARIANTS
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    name = a.workload
+    cls = VARIANTS[WORKLOADS[name][4]]
+    p = make_problem(name)
+    s = cls(p)
+    s.set_populations(initial_state(name, seed=rank))
+    L = a.lbm_steps
+    nodes = p.n_nodes
+
+    def barrier() -> None:
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---------------- device-resident throughput
+    for _ in range(a.warmup):
+        s.step(L)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record()
+        for _ in range(a.steps):
+            s.step(L)
+        ev1.record()
+        ev1.synchronize()
+    barrier()
+    dt = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    clocks = clk.summary()
+    launches = a.steps * L  # one kernel launch per lattice time step (AB and AA alike)
+    value = world * nodes * L * a.steps / dt / 1e6
+
+    # ---------------- end to end through the solver API, host buffers
+    e2e = None
+    if not a.no_e2e:
+        host_in = torch.empty(s.A.numel(), dtype=s.A.dtype, pin_memory=True)
+        host_in.copy_(s.A)
+        host_out = torch.empty_like(host_in, pin_memory=True)
+        for _ in range(1):
+            s.A.copy_(host_in, non_blocking=True)
+            s.step(L)
+            host_out.copy_(s.A, non_blocking=True)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            s.A.copy_(host_in, non_blocking=True)
+            s.step(L)
+            host_out.copy_(s.A, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        barrier()
+        dte = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        nbytes = s.A.numel() * s.A.element_size()
+        e2e = {"value": world * nodes * L * a.steps / dte / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        bpn = s.bytes_per_node
+        achieved = bpn * nodes / (dt / launches) / 1e9
+        tag = f"{name}"
+        traffic = traffic_from_profiles(tag)
+        out = {
+            "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if s.storage == "f32" else s.storage, "data": "synthetic",
+            "config": config_of(name, a),
+            "bytes_per_update": bpn, "effective_GBs": value * 1e6 * bpn / 1e9,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": bpn * nodes},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if e2e is not None:
+            out["e2e"] = e2e
+        if world == 1 and not a.no_cpu:
+            out["cpu_baseline"] = cpu_baseline(name)
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="d2q9-bgk-ab-f32", choices=sorted(WORKLOADS))
+    ap.add_argument("--lbm-steps", type=int, default=1000,
+                    help="lattice time steps per benchmark step")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-procs", type=int, default=64)
+    a = ap.parse_args()
+    if a.warmup < 3 and a.impl == "b200":
+        log("note: fewer than 3 warm-up steps")
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,141 @@
+/*
+ * pylbm_b200 -- C ABI of the B200 (sm_100a) fused lattice-Boltzmann stream-collide library.
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream handle (cast to uint64_t);
+ * no torch or C++ types cross this boundary. Device buffers are owned by the caller and are
+ * never freed by the library. Launches are asynchronous on the given stream.
+ *
+ * Return value of every int-returning call: 0 on success, a negative LBM_E_* code for an
+ * invalid argument (nothing was launched), or a positive cudaError_t value when the CUDA
+ * runtime reported an error. lbm_error_string() turns any of them into text.
+ *
+ * Layouts (identical to pylbm's):
+ *   population buffer: structure of arrays, element (i, n) at index i * N + n,
+ *   n = x + nx * (y + ny * z), N = nx * ny * nz, q planes (9 for D2Q9, 19 for D3Q19).
+ *   Velocity orders, weights and opposite tables follow pylbm's lattice.py:
+ *     D2Q9  0 rest, 1 E, 2 N, 3 W, 4 S, 5 NE, 6 NW, 7 SW, 8 SE
+ *     D3Q19 0 rest, then opposite pairs adjacent: (1,2) (3,4) ... (17,18)
+ *   The stored value is f (LBM_STORE_F32) or f - w_i (the three shifted storages).
+ *   AA-pattern buffers between step pairs hold population i in slot opp(i).
+ */
+#ifndef PYLBM_B200_H
+#define PYLBM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* lattices */
+#define LBM_D2Q9 0
+#define LBM_D3Q19 1
+/* collision operators */
+#define LBM_BGK 0
+#define LBM_TRT 1
+#define LBM_MRT 2 /* D2Q9 only */
+#define LBM_STREAM_ONLY 3 /* debug: streaming and boundaries only, no collision */
+/* storage formats; arithmetic is fp32 in every case */
+#define LBM_STORE_F32 0         /* f in fp32, unshifted arithmetic (pylbm's own fp32 scheme) */
+#define LBM_STORE_F16 1         /* f - w_i in fp16, shifted arithmetic */
+#define LBM_STORE_BF16 2        /* f - w_i in bf16, shifted arithmetic */
+#define LBM_STORE_F32_SHIFTED 3 /* f - w_i in fp32, shifted arithmetic */
+/* streaming patterns */
+#define LBM_PATTERN_AB 0      /* pull, reads src, writes dst (src != dst) */
+#define LBM_PATTERN_AA_ODD 1  /* in place: reads swapped layout, writes natural layout */
+#define LBM_PATTERN_AA_EVEN 2 /* in place: reads natural layout, writes swapped layout */
+/* buffer layouts for the read-only helpers */
+#define LBM_LAYOUT_NATURAL 0
+#define LBM_LAYOUT_AA_SWAPPED 1
+
+/* error codes (negative; positive values are cudaError_t) */
+#define LBM_OK 0
+#define LBM_E_NULL -1        /* a required pointer is NULL */
+#define LBM_E_LATTICE -2     /* unknown lattice id */
+#define LBM_E_COLLISION -3   /* unknown collision, or MRT on D3Q19 */
+#define LBM_E_STORAGE -4     /* unknown storage id */
+#define LBM_E_PATTERN -5     /* unknown pattern id */
+#define LBM_E_SHAPE -6       /* a dimension < 1, or nz != 1 for D2Q9 */
+#define LBM_E_INDEX -7       /* q * N does not fit in int32 (pylbm's fused-kernel limit) */
+#define LBM_E_RATE -8        /* a relaxation rate or force is not finite, or rate outside (0, 2) */
+#define LBM_E_LID -9         /* moving lid requested on a periodic last axis */
+#define LBM_E_ALIGN -10      /* a device pointer is not aligned to its element size (16 B for buffers) */
+#define LBM_E_ALIAS -11      /* AB pattern with src == dst, or AA pattern with src != dst */
+#define LBM_E_STEPS -12      /* negative step count, or odd count for the AA pattern */
+#define LBM_E_TIMEOUT -13    /* a bounded device-side wait gave up (error flag set by the kernel) */
+#define LBM_E_HANDLE -14     /* unknown or destroyed handle */
+#define LBM_E_ARG -15        /* any other invalid argument */
+#define LBM_E_SIZE -16       /* problem larger than a fixed capacity */
+
+/* Problem descriptor: the compile-time #defines and runtime scalars of pylbm's fused kernel
+ * (backends/cupy_backend.py:51-70 header, backends/_fused.py:129-136 scalar_args) as one POD.
+ * Rates follow codegen.py:437-445 runtime_rates: BGK r0 = 1/tau; TRT r0 = s+, r1 = s-;
+ * MRT r0 = s_nu, r1 = s_e, r2 = s_eps, r3 = s_q. */
+typedef struct LbmDesc {
+    int32_t lattice;
+    int32_t collision;
+    int32_t storage;
+    int32_t periodic_mask; /* bit a set: axis a (0 = x, 1 = y, 2 = z) is periodic, else walls */
+    int32_t nx, ny, nz;    /* nz = 1 for D2Q9 */
+    float ulid;            /* lid speed: top wall of the last axis moving in +x; 0 = no lid */
+    float fx, fy, fz;      /* uniform Guo body force (fz ignored in 2D) */
+    float r0, r1, r2, r3;  /* relaxation rates, see above */
+    /* optional extensions beyond pylbm's fused kernel (NULL = off) */
+    const uint32_t* solid_bits; /* 1 bit per node: bit (n & 31) of word (n >> 5); solid nodes
+                                   act as stationary half-way bounce-back obstacles */
+    const float* force_field;   /* per-node force added to (fx, fy, fz): layout (d, N) fp32 */
+    double* mx_force;           /* momentum-exchange force on the solids, added (not stored)
+                                   into mx_force[0..d-1] by each step that writes a state */
+    int64_t mx_stride;          /* doubles between the slots of consecutive steps in
+                                   lbm_advance (0 = every step adds into the same slot) */
+} LbmDesc;
+
+/* Library identification. */
+int lbm_abi_version(void);
+const char* lbm_error_string(int code);
+
+/* Host-only: the lattice tables compiled into the kernels (c as q rows of 3, w, opp), so a
+ * caller can check them against pylbm's lattice.py:49-67 without a GPU. */
+int lbm_lattice_info(int lattice, int* q, int* dim, int* c, double* w, int* opp);
+
+/* Host-only validation of a descriptor (no GPU needed). Same checks as the launch paths:
+ * pylbm's capability gate backends/_fused.py:54-66 (q*N < 2^31) and problem.py:44-61. */
+int lbm_validate(const LbmDesc* d);
+
+/* One fused stream-collide launch of the given pattern.
+ * Replaces FusedSolver._launch (backends/_fused.py:112-114, cupy_backend.py:101-103):
+ * 'ab' reads src and writes dst; 'aa-odd' / 'aa-even' update src in place (dst == src). */
+int lbm_launch(const LbmDesc* d, const void* src, void* dst, int pattern, uint64_t stream);
+
+/* Advance nsteps time steps. Replaces FusedSolver._advance (backends/_fused.py:116-124).
+ * aa = 0: pull two-buffer; step k reads (k even ? a : b) and writes the other buffer, so the
+ *         result is in a when nsteps is even and in b when it is odd.
+ * aa = 1: AA in place on a (b ignored); nsteps must be even (odd + even launch per pair). */
+int lbm_advance(const LbmDesc* d, void* a, void* b, int aa, int nsteps, uint64_t stream);
+
+/* FP64 global sums of a stored state: out[0] = sum rho (mass), out[1..d] = sum c f
+ * (momentum), written to DEVICE memory out[0..d]. Deterministic two-pass reduction.
+ * No pylbm counterpart as a kernel; the host equivalent is core.py:255-266 summed. */
+int lbm_moments_f64(const LbmDesc* d, const void* f, int layout, double* out,
+                    uint64_t stream);
+
+/* Device macroscopic fields from a stored state: rho[N], u[d * N] (fp32), with the physical
+ * velocity u = (sum c f - F/2) / rho of pylbm's core.macroscopic (core.py:255-266). */
+int lbm_macroscopic(const LbmDesc* d, const void* f, int layout, float* rho, float* u,
+                    uint64_t stream);
+
+/* Canonical float64 populations (q, N) <-> stored buffer, on the device.
+ * Replaces FusedSolver._encode / populations (backends/_fused.py:83-103): subtracts or adds
+ * w_i for shifted storages and applies the AA slot swap when layout = LBM_LAYOUT_AA_SWAPPED. */
+int lbm_encode_f64(const LbmDesc* d, const double* f64, void* buf, int layout,
+                   uint64_t stream);
+int lbm_decode_f64(const LbmDesc* d, const void* buf, int layout, double* f64,
+                   uint64_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYLBM_B200_H */

@@ -1,0 +1,43 @@
+// Host-side launchers shared between translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/pylbm_b200.h"
+#include "params.cuh"
+
+namespace lbm {
+
+// True when the step needs the Guo source terms.
+inline bool needs_force(const LbmDesc& d) {
+    return d.fx != 0.0f || d.fy != 0.0f || (d.lattice == LBM_D3Q19 && d.fz != 0.0f) ||
+           d.force_field != nullptr;
+}
+
+inline int block_x_for(int nx) {
+    for (int b : {128, 64, 32})
+        if (nx % b == 0) return b;
+    return 128;
+}
+
+// One launch of the generic kernel (step_generic_*.cu). Arguments are validated.
+int launch_generic_d2q9(const LbmDesc& d, const void* src, void* dst, int pattern,
+                        cudaStream_t s);
+int launch_generic_d3q19(const LbmDesc& d, const void* src, void* dst, int pattern,
+                         cudaStream_t s);
+
+// Specialised kernels; each returns 1 when it does not handle the case (the caller then
+// uses the generic kernel), else 0 or a cudaError_t.
+int launch_fast_d2q9(const LbmDesc& d, const void* src, void* dst, int pattern,
+                     cudaStream_t s);
+int launch_fast_d3q19(const LbmDesc& d, const void* src, void* dst, int pattern,
+                      cudaStream_t s);
+
+// Helpers (helpers.cu)
+int launch_encode(const LbmDesc& d, const double* f64, void* buf, int layout, cudaStream_t s);
+int launch_decode(const LbmDesc& d, const void* buf, int layout, double* f64, cudaStream_t s);
+int launch_macroscopic(const LbmDesc& d, const void* f, int layout, float* rho, float* u,
+                       cudaStream_t s);
+int launch_moments(const LbmDesc& d, const void* f, int layout, double* out, cudaStream_t s);
+
+}  // namespace lbm
