@@ -26,7 +26,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -78,19 +77,21 @@ def traffic_from_profiles(kernel_tag: str) -> float | None:
         return None
 
 
-def make_problem(name: str):
+def make_problem(name: str, n: int | None = None):
     from pylbm_b200.problem import Problem
 
-    lat, n, coll, tau, _ = WORKLOADS[name]
+    lat, n0, coll, tau, _ = WORKLOADS[name]
+    n = n or n0
     if lat == "D2Q9":
         return Problem((n, n), tau=tau, collision=coll, periodic=(True, True))
     return Problem((n, n, n), tau=tau, collision=coll, periodic=(True, True, True))
 
 
-def initial_state(name: str, seed: int) -> np.ndarray:
+def initial_state(name: str, seed: int, n: int | None = None) -> np.ndarray:
     from pylbm_b200 import workloads as W
 
-    lat, n, *_ = WORKLOADS[name]
+    lat, n0, *_ = WORKLOADS[name]
+    n = n or n0
     if lat == "D2Q9":
         return W.fourier_populations(n, seed)
     return W.taylor_green_3d_populations(n)
@@ -227,6 +228,7 @@ def run_reference(a: argparse.Namespace) -> None:
 
 def config_of(name: str, a: argparse.Namespace) -> dict:
     lat, n, coll, tau, variant = WORKLOADS[name]
+    n = a.n or n
     shape = [n, n] if lat == "D2Q9" else [n, n, n]
     return {"workload": name, "lattice": lat, "shape": shape, "collision": coll, "tau": tau,
             "variant": variant, "periodic": True, "lbm_steps_per_step": a.lbm_steps,
@@ -252,9 +254,9 @@ def run_b200(a: argparse.Namespace) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     name = a.workload
     cls = VARIANTS[WORKLOADS[name][4]]
-    p = make_problem(name)
+    p = make_problem(name, a.n)
     s = cls(p)
-    s.set_populations(initial_state(name, seed=rank))
+    s.set_populations(initial_state(name, seed=rank, n=a.n))
     L = a.lbm_steps
     nodes = p.n_nodes
 
@@ -351,6 +353,7 @@ def main() -> None:
     ap.add_argument("--workload", default="d2q9-bgk-ab-f32", choices=sorted(WORKLOADS))
     ap.add_argument("--lbm-steps", type=int, default=1000,
                     help="lattice time steps per benchmark step")
+    ap.add_argument("--n", type=int, default=None, help="override the lattice edge (profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=64)

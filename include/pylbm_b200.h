@@ -90,7 +90,12 @@ typedef struct LbmDesc {
                                    into mx_force[0..d-1] by each step that writes a state */
     int64_t mx_stride;          /* doubles between the slots of consecutive steps in
                                    lbm_advance (0 = every step adds into the same slot) */
+    int32_t flags;              /* LBM_FLAG_* bits, 0 by default */
+    int32_t reserved;
 } LbmDesc;
+
+/* descriptor flags */
+#define LBM_FLAG_GENERIC 1 /* always use the one-node-per-thread kernel (for A/B testing) */
 
 /* Library identification. */
 int lbm_abi_version(void);

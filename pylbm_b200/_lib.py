@@ -19,6 +19,7 @@ STORE_F32, STORE_F16, STORE_BF16, STORE_F32_SHIFTED = 0, 1, 2, 3
 PATTERN_AB, PATTERN_AA_ODD, PATTERN_AA_EVEN = 0, 1, 2
 LAYOUT_NATURAL, LAYOUT_AA_SWAPPED = 0, 1
 E_TIMEOUT = -13
+FLAG_GENERIC = 1
 
 
 class LbmDesc(ctypes.Structure):
@@ -42,6 +43,8 @@ class LbmDesc(ctypes.Structure):
         ("force_field", ctypes.c_void_p),
         ("mx_force", ctypes.c_void_p),
         ("mx_stride", ctypes.c_int64),
+        ("flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

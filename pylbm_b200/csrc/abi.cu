@@ -27,6 +27,9 @@ bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p
 cudaStream_t as_stream(uint64_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
 int launch_one(const LbmDesc& d, const void* src, void* dst, int pattern, cudaStream_t s) {
+    if (d.flags & LBM_FLAG_GENERIC)
+        return d.lattice == LBM_D2Q9 ? launch_generic_d2q9(d, src, dst, pattern, s)
+                                     : launch_generic_d3q19(d, src, dst, pattern, s);
     const int fast = d.lattice == LBM_D2Q9 ? launch_fast_d2q9(d, src, dst, pattern, s)
                                            : launch_fast_d3q19(d, src, dst, pattern, s);
     if (fast != 1) return fast;

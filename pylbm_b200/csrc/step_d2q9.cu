@@ -1,9 +1,361 @@
-// Specialised D2Q9 kernels (vectorised rows). Not yet specialised: every case goes to the
-// generic kernel.
+// Vectorised D2Q9 kernels: every lane owns V consecutive nodes of one row (V = 4 fp32 or
+// 8 x 16-bit, one 16-byte vector per population plane).
+//
+// Pull (AB and the read half of AA-odd): the row segment of plane i is read at row y - c_iy
+// with one aligned 16-byte load; the x-shift by c_ix moves elements inside the vector and
+// takes the element across the lane boundary from the neighbouring lane with one warp
+// shuffle. Only the first and last lane of a warp read one more element (the warp's halo) with
+// a scalar load that the neighbouring warp's line already brought into L2; warps are
+// otherwise independent (no shared memory, no block barrier). x walls and the periodic x wrap
+// are resolved inside that halo element.
+//
+// Rows next to a y wall (y = 0 and y = ny - 1 of a non-periodic y axis) take a separate,
+// general code path (the whole segment bounces back from the node's own opposite plane, plus
+// the lid term on the top wall); every other row runs a path with no wall or lid code at all.
+// The branch is uniform per block, and keeping the wall logic out of the hot path keeps its
+// nine loads in flight together (measured: the fused variant ran 20% slower otherwise).
+//
+// AA-odd push: the write of p_i(x) to x + c_i is an aligned vector store of the segment
+// shifted by one element, except at warp edges. The AA scheme is race-free because every
+// memory slot is read and written by one node only (slot (i, x + c_i) belongs to node x); so
+// a lane stores an aligned vector only when all of its elements belong to nodes of its own
+// warp, and the first / last lane stores the slots of its own nodes one element at a time.
+//
+// Semantics are those of the generic kernel (step_generic.cuh) and of pylbm's fused kernel
+// (lbm.cu:71-198, codegen.py:10-16); the collision is the shared collide<>().
+#include "codec.cuh"
+#include "collide.cuh"
 #include "dispatch.cuh"
+#include "lattice.cuh"
+#include "params.cuh"
+#include "vec.cuh"
 
 namespace lbm {
+namespace {
 
-int launch_fast_d2q9(const LbmDesc&, const void*, void*, int, cudaStream_t) { return 1; }
+using L = D2Q9;
+constexpr int kThreads = 128;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Lid term 6 w_i c_ix U for a pull whose source is behind the top wall.
+__device__ __forceinline__ float lid_term(int i, float ulid) {
+    return 6.0f * L::w(i) * float(L::cx(i)) * ulid;
+}
+
+// Row y - cy, wrapped. EDGE rows also report whether the row lies behind a wall (then it is
+// not wrapped) and whether that wall is the top one.
+template <bool EDGE>
+__device__ __forceinline__ int src_row(int y, int cy, int ny, bool per, bool& wall, bool& top) {
+    int ys = y - cy;
+    wall = top = false;
+    if constexpr (!EDGE) {
+        ys += ys < 0 ? ny : (ys >= ny ? -ny : 0);
+    } else if (ys < 0 || ys >= ny) {
+        if (per) {
+            ys += ys < 0 ? ny : -ny;
+        } else {
+            wall = true;
+            top = ys >= ny;
+        }
+    }
+    return ys;
+}
+
+// Load the pulled row segments of all 9 directions into v[] (raw storage elements), already
+// shifted along x. READ_OPP selects the AA-odd reading (source slot opp(i), bounce-back slot
+// i) instead of the two-buffer one (source slot i, bounce-back slot opp(i)).
+template <int STORE, bool READ_OPP, bool NC, bool EDGE>
+__device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT<STORE>::E* A,
+                                          int x0, int y, bool active, bool first, bool last,
+                                          uint4 (&v)[9], float (&lid)[9]) {
+    using E = typename VT<STORE>::E;
+    constexpr int V = VT<STORE>::V;
+    const int nx = P.n[0], ny = P.n[1], N = P.N;
+    const bool perx = P.per[0], pery = P.per[1];
+    uint32_t halo[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int cx = L::cx(i), cy = L::cy(i);
+        const int src_slot = READ_OPP ? L::opp(i) : i;
+        const int bb_slot = READ_OPP ? i : L::opp(i);
+        bool wall, top;
+        const int ys = src_row<EDGE>(y, cy, ny, pery, wall, top);
+        lid[i] = (wall && top && cx != 0) ? lid_term(i, P.ulid) : 0.0f;
+        v[i] = make_uint4(0u, 0u, 0u, 0u);
+        halo[i] = 0u;
+        if (!active) continue;
+        if (wall) {  // the whole segment bounces back from the node's own opposite slot
+            const E* p = A + bb_slot * N + y * nx + x0;
+            v[i] = NC ? ld_nc(p) : ld_plain(p);
+            continue;
+        }
+        const E* row = A + src_slot * N + ys * nx;
+        v[i] = NC ? ld_nc(row + x0) : ld_plain(row + x0);
+        if (cx == 1 && first) {
+            const E* h = x0 > 0 ? row + x0 - 1
+                                : (perx ? row + nx - 1 : A + bb_slot * N + y * nx);
+            halo[i] = NC ? ld1_nc(h) : ld1(h);
+        }
+        if (cx == -1 && last) {
+            const E* h = x0 + V < nx ? row + x0 + V
+                                     : (perx ? row : A + bb_slot * N + y * nx + nx - 1);
+            halo[i] = NC ? ld1_nc(h) : ld1(h);
+        }
+    }
+    // x-shifts: element k of node x0 + k comes from x0 + k - cx
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int cx = L::cx(i);
+        if (cx == 0) continue;
+        bool wall, top;
+        src_row<EDGE>(y, L::cy(i), ny, pery, wall, top);
+        if (cx == 1) {
+            uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
+            if (first) up = halo[i];
+            if (!wall) {
+#pragma unroll
+                for (int k = V - 1; k > 0; --k) put<V>(v[i], k, elem<V>(v[i], k - 1));
+                put<V>(v[i], 0, up);
+            }
+        } else {
+            uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
+            if (last) dn = halo[i];
+            if (!wall) {
+#pragma unroll
+                for (int k = 0; k < V - 1; ++k) put<V>(v[i], k, elem<V>(v[i], k + 1));
+                put<V>(v[i], V - 1, dn);
+            }
+        }
+    }
+}
+
+// Collide the V nodes of the lane in place (raw elements in, raw elements out). With LIDS,
+// lid[i] is added to the pulled value of direction i and sub[i] is subtracted from its
+// post-collision value before it is stored (the AA-odd push into the lid).
+template <int STORE, int COLL, bool FORCE, bool LIDS>
+__device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[9],
+                                             const float (&lid)[9], const float (&sub)[9]) {
+    using T = VT<STORE>;
+    constexpr int V = T::V;
+    constexpr bool SHIFT = Codec<STORE>::shifted;
+    const float F[3] = {P.F[0], P.F[1], 0.0f};
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        float f[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            f[i] = T::f(elem<V>(v[i], k));
+            if (LIDS) f[i] += lid[i];
+        }
+        collide<L, COLL, SHIFT, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) put<V>(v[i], k, T::b(LIDS ? f[i] - sub[i] : f[i]));
+    }
+}
+
+struct Lane {
+    int x0, y, lane;
+    bool active, first, last;
+};
+
+template <int STORE>
+__device__ __forceinline__ Lane lane_of(const StepParams& P) {
+    constexpr int V = VT<STORE>::V;
+    Lane l;
+    l.lane = threadIdx.x & 31;
+    l.x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+    l.y = blockIdx.y;
+    l.active = l.x0 < P.n[0];
+    l.first = l.lane == 0;
+    l.last = l.active && (l.lane == 31 || l.x0 + V >= P.n[0]);
+    return l;
+}
+
+// A row next to a y wall (only those carry wall and lid logic).
+__device__ __forceinline__ bool edge_row(const StepParams& P, int y) {
+    return !P.per[1] && (y == 0 || y == P.n[1] - 1);
+}
+
+template <int STORE, int COLL, bool FORCE, bool EDGE>
+__device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<STORE>::E* A,
+                                       typename VT<STORE>::E* B, const Lane& l) {
+    uint4 v[9];
+    float lid[9];
+    pull_rows<STORE, false, true, EDGE>(P, A, l.x0, l.y, l.active, l.first, l.last, v, lid);
+    if (!l.active) return;
+    const float zero[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid, zero);
+    const int n0 = l.y * P.n[0] + l.x0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) st_cs(B + i * P.N + n0, v[i]);
+}
+
+template <int STORE, int COLL, bool FORCE>
+__global__ void __launch_bounds__(kThreads)
+k_d2q9_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
+    using E = typename VT<STORE>::E;
+    const E* __restrict__ A = static_cast<const E*>(Av);
+    E* __restrict__ B = static_cast<E*>(Bv);
+    const Lane l = lane_of<STORE>(P);
+    if (edge_row(P, l.y)) ab_row<STORE, COLL, FORCE, true>(P, A, B, l);
+    else ab_row<STORE, COLL, FORCE, false>(P, A, B, l);
+}
+
+template <int STORE, int COLL, bool FORCE>
+__global__ void __launch_bounds__(kThreads)
+k_d2q9_aa_even(const StepParams P, void* Av) {
+    using E = typename VT<STORE>::E;
+    constexpr int V = VT<STORE>::V;
+    E* A = static_cast<E*>(Av);
+    const int n0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+    if (n0 >= P.N) return;
+    uint4 v[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) v[i] = ld_plain(A + i * P.N + n0);
+    const float zero[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    collide_lane<STORE, COLL, FORCE, false>(P, v, zero, zero);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) st_cs(A + L::opp(i) * P.N + n0, v[i]);
+}
+
+template <int STORE, int COLL, bool FORCE, bool EDGE>
+__device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STORE>::E* A,
+                                           const Lane& l) {
+    using E = typename VT<STORE>::E;
+    constexpr int V = VT<STORE>::V;
+    const int nx = P.n[0], ny = P.n[1], N = P.N;
+    uint4 v[9];
+    float lid[9];
+    pull_rows<STORE, true, false, EDGE>(P, A, l.x0, l.y, l.active, l.first, l.last, v, lid);
+    // destinations x + c_i: whole-row wall bounces carry the lid term with the push sign
+    float sub[9];
+    bool dwall[9];
+    int drow[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        bool wall, top;
+        drow[i] = src_row<EDGE>(l.y, -L::cy(i), ny, P.per[1], wall, top);
+        dwall[i] = wall;
+        sub[i] = (wall && top && L::cx(i) != 0) ? lid_term(i, P.ulid) : 0.0f;
+    }
+    if (l.active) collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid, sub);
+    const int own = l.y * nx + l.x0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int cx = L::cx(i);
+        E* plane = A + i * N + drow[i] * nx;
+        E* bb = A + L::opp(i) * N + l.y * nx;  // own row, opposite slot
+        if (dwall[i]) {
+            if (l.active) st_plain(A + L::opp(i) * N + own, v[i]);
+            continue;
+        }
+        if (cx == 0) {
+            if (l.active) st_plain(plane + l.x0, v[i]);
+        } else if (cx == 1) {
+            const uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
+            if (!l.active) continue;
+            if (!l.first) {
+                uint4 w;
+                put<V>(w, 0, up);
+#pragma unroll
+                for (int k = 1; k < V; ++k) put<V>(w, k, elem<V>(v[i], k - 1));
+                st_plain(plane + l.x0, w);
+            } else {
+#pragma unroll
+                for (int k = 0; k < V - 1; ++k) st1(plane + l.x0 + 1 + k, elem<V>(v[i], k));
+            }
+            if (l.last) {
+                E* dst = l.x0 + V < nx ? plane + l.x0 + V
+                                       : (P.per[0] ? plane : bb + nx - 1);
+                st1(dst, elem<V>(v[i], V - 1));
+            }
+        } else {
+            const uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
+            if (!l.active) continue;
+            if (!l.last) {
+                uint4 w;
+#pragma unroll
+                for (int k = 0; k < V - 1; ++k) put<V>(w, k, elem<V>(v[i], k + 1));
+                put<V>(w, V - 1, dn);
+                st_plain(plane + l.x0, w);
+            } else {
+#pragma unroll
+                for (int k = 1; k < V; ++k) st1(plane + l.x0 + k - 1, elem<V>(v[i], k));
+            }
+            if (l.first) {
+                E* dst = l.x0 > 0 ? plane + l.x0 - 1 : (P.per[0] ? plane + nx - 1 : bb);
+                st1(dst, elem<V>(v[i], 0));
+            }
+        }
+    }
+}
+
+template <int STORE, int COLL, bool FORCE>
+__global__ void __launch_bounds__(kThreads)
+k_d2q9_aa_odd(const StepParams P, void* Av) {
+    using E = typename VT<STORE>::E;
+    E* A = static_cast<E*>(Av);
+    const Lane l = lane_of<STORE>(P);
+    if (edge_row(P, l.y)) aa_odd_row<STORE, COLL, FORCE, true>(P, A, l);
+    else aa_odd_row<STORE, COLL, FORCE, false>(P, A, l);
+}
+
+template <int STORE, int COLL, bool FORCE>
+int go(const StepParams& P, const void* src, void* dst, int pattern, cudaStream_t s) {
+    constexpr int V = VT<STORE>::V;
+    if (pattern == LBM_PATTERN_AA_EVEN) {
+        const int threads = P.N / V;
+        k_d2q9_aa_even<STORE, COLL, FORCE>
+            <<<(threads + kThreads - 1) / kThreads, kThreads, 0, s>>>(P, dst);
+        return int(cudaGetLastError());
+    }
+    const int per_row = P.n[0] / V;
+    const dim3 grid((per_row + kThreads - 1) / kThreads, P.n[1]);
+    if (pattern == LBM_PATTERN_AB)
+        k_d2q9_ab<STORE, COLL, FORCE><<<grid, kThreads, 0, s>>>(P, src, dst);
+    else
+        k_d2q9_aa_odd<STORE, COLL, FORCE><<<grid, kThreads, 0, s>>>(P, dst);
+    return int(cudaGetLastError());
+}
+
+template <int STORE, int COLL>
+int go_f(const LbmDesc& d, const StepParams& P, const void* src, void* dst, int pattern,
+         cudaStream_t s) {
+    return needs_force(d) ? go<STORE, COLL, true>(P, src, dst, pattern, s)
+                          : go<STORE, COLL, false>(P, src, dst, pattern, s);
+}
+
+template <int STORE>
+int go_c(const LbmDesc& d, const StepParams& P, const void* src, void* dst, int pattern,
+         cudaStream_t s) {
+    switch (d.collision) {
+        case LBM_BGK: return go_f<STORE, LBM_BGK>(d, P, src, dst, pattern, s);
+        case LBM_TRT: return go_f<STORE, LBM_TRT>(d, P, src, dst, pattern, s);
+        case LBM_MRT: return go_f<STORE, LBM_MRT>(d, P, src, dst, pattern, s);
+        case LBM_STREAM_ONLY: return go<STORE, LBM_STREAM_ONLY, false>(P, src, dst, pattern, s);
+    }
+    return LBM_E_COLLISION;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+int launch_fast_d2q9(const LbmDesc& d, const void* src, void* dst, int pattern,
+                     cudaStream_t s) {
+    // the vector kernels cover box problems whose rows split into whole 16-byte vectors
+    if (d.solid_bits || d.force_field || d.mx_force) return 1;
+    const int V = (d.storage == LBM_STORE_F16 || d.storage == LBM_STORE_BF16) ? 8 : 4;
+    if (d.nx % V != 0) return 1;
+    if (!aligned16(src) || !aligned16(dst)) return 1;
+    const StepParams P = make_params(d);
+    switch (d.storage) {
+        case LBM_STORE_F32: return go_c<LBM_STORE_F32>(d, P, src, dst, pattern, s);
+        case LBM_STORE_F32_SHIFTED: return go_c<LBM_STORE_F32_SHIFTED>(d, P, src, dst, pattern, s);
+        case LBM_STORE_F16: return go_c<LBM_STORE_F16>(d, P, src, dst, pattern, s);
+        case LBM_STORE_BF16: return go_c<LBM_STORE_BF16>(d, P, src, dst, pattern, s);
+    }
+    return LBM_E_STORAGE;
+}
 
 }  // namespace lbm

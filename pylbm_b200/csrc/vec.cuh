@@ -1,0 +1,106 @@
+// 16-byte vectors of stored populations: 4 fp32 or 8 fp16 / bf16 elements per uint4.
+//
+// Elements are handled as raw bit patterns (uint32 holding 32 or 16 bits) so that the x-shift
+// of a row segment is a register permutation plus one warp shuffle, independent of the type;
+// conversion to fp32 happens once per node, right before the collision.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstdint>
+
+#include "../../include/pylbm_b200.h"
+
+namespace lbm {
+
+template <int STORE>
+struct VT;
+
+template <>
+struct VT<LBM_STORE_F32> {
+    using E = uint32_t;
+    static constexpr int V = 4;
+    __device__ __forceinline__ static float f(uint32_t b) { return __uint_as_float(b); }
+    __device__ __forceinline__ static uint32_t b(float v) { return __float_as_uint(v); }
+};
+template <>
+struct VT<LBM_STORE_F32_SHIFTED> : VT<LBM_STORE_F32> {};
+
+template <>
+struct VT<LBM_STORE_F16> {
+    using E = uint16_t;
+    static constexpr int V = 8;
+    __device__ __forceinline__ static float f(uint32_t b) {
+        return __half2float(__ushort_as_half(static_cast<unsigned short>(b)));
+    }
+    __device__ __forceinline__ static uint32_t b(float v) {
+        return __half_as_ushort(__float2half_rn(v));
+    }
+};
+
+template <>
+struct VT<LBM_STORE_BF16> {
+    using E = uint16_t;
+    static constexpr int V = 8;
+    __device__ __forceinline__ static float f(uint32_t b) { return __uint_as_float(b << 16); }
+    __device__ __forceinline__ static uint32_t b(float v) {
+        return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+    }
+};
+
+__device__ __forceinline__ uint32_t word(const uint4& v, int j) {
+    return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void set_word(uint4& v, int j, uint32_t w) {
+    if (j == 0) v.x = w;
+    else if (j == 1) v.y = w;
+    else if (j == 2) v.z = w;
+    else v.w = w;
+}
+
+// element k (compile-time after unrolling) of a vector of V elements
+template <int V>
+__device__ __forceinline__ uint32_t elem(const uint4& v, int k) {
+    if constexpr (V == 4) return word(v, k);
+    else return (word(v, k >> 1) >> ((k & 1) * 16)) & 0xffffu;
+}
+template <int V>
+__device__ __forceinline__ void put(uint4& v, int k, uint32_t e) {
+    if constexpr (V == 4) {
+        set_word(v, k, e);
+    } else {
+        const uint32_t w = word(v, k >> 1);
+        set_word(v, k >> 1, (k & 1) ? ((w & 0x0000ffffu) | (e << 16)) : ((w & 0xffff0000u) | e));
+    }
+}
+
+// Whole-vector moves.
+__device__ __forceinline__ uint4 ld_nc(const void* p) {
+    return __ldg(reinterpret_cast<const uint4*>(p));
+}
+__device__ __forceinline__ uint4 ld_plain(const void* p) {
+    return *reinterpret_cast<const uint4*>(p);
+}
+__device__ __forceinline__ void st_cs(void* p, const uint4& v) {
+    __stcs(reinterpret_cast<uint4*>(p), v);
+}
+__device__ __forceinline__ void st_plain(void* p, const uint4& v) {
+    *reinterpret_cast<uint4*>(p) = v;
+}
+
+// Single elements.
+template <class E>
+__device__ __forceinline__ uint32_t ld1_nc(const E* p) {
+    return uint32_t(__ldg(p));
+}
+template <class E>
+__device__ __forceinline__ uint32_t ld1(const E* p) {
+    return uint32_t(*p);
+}
+template <class E>
+__device__ __forceinline__ void st1(E* p, uint32_t e) {
+    *p = static_cast<E>(e);
+}
+
+}  // namespace lbm
