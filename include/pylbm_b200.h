@@ -96,6 +96,7 @@ typedef struct LbmDesc {
 
 /* descriptor flags */
 #define LBM_FLAG_GENERIC 1 /* always use the one-node-per-thread kernel (for A/B testing) */
+#define LBM_FLAG_STAGED 2  /* D2Q9: use the TMA-staged kernel instead of the register one */
 
 /* Library identification. */
 int lbm_abi_version(void);
@@ -138,6 +139,24 @@ int lbm_encode_f64(const LbmDesc* d, const double* f64, void* buf, int layout,
                    uint64_t stream);
 int lbm_decode_f64(const LbmDesc* d, const void* buf, int layout, double* f64,
                    uint64_t stream);
+
+/* Tuning of the TMA-staged kernels (D3Q19 always; D2Q9 with LBM_FLAG_STAGED), per lattice and
+ * stored element size (2 or 4 bytes), process-wide: nodes per row segment (multiple of 8),
+ * shared-memory ring depth (2..8) and consumer warps (1..8). No pylbm counterpart (pylbm
+ * launches one fixed block shape, _fused.py:26-31); used by the autotuner. */
+int lbm_set_staged_config(int lattice, int elem_bytes, int width, int stages, int warps);
+int lbm_get_staged_config(int lattice, int elem_bytes, int* width, int* stages, int* warps);
+
+/* Synchronise the current device and report its device error word: LBM_OK, or LBM_E_TIMEOUT
+ * when a kernel's bounded wait gave up since the last clear (clear != 0 resets the word). */
+int lbm_device_error(int clear);
+
+/* Failure-detection self test (D3Q19 descriptor, any 16-byte aligned buffer that is left
+ * untouched): launches the staged kernel with its copy producer disabled, so every consumer
+ * wait runs out after timeout_ns (0 < timeout_ns <= 10 s); lbm_device_error() then reports
+ * LBM_E_TIMEOUT and the context stays usable. */
+int lbm_selftest_wait_timeout(const LbmDesc* d, void* buf, uint64_t timeout_ns,
+                              uint64_t stream);
 
 #ifdef __cplusplus
 }

@@ -20,6 +20,7 @@ PATTERN_AB, PATTERN_AA_ODD, PATTERN_AA_EVEN = 0, 1, 2
 LAYOUT_NATURAL, LAYOUT_AA_SWAPPED = 0, 1
 E_TIMEOUT = -13
 FLAG_GENERIC = 1
+FLAG_STAGED = 2
 
 
 class LbmDesc(ctypes.Structure):
@@ -71,6 +72,10 @@ _SIGNATURES = {
     "lbm_macroscopic": ([_d, _vp, _i, _vp, _vp, _u64], _i),
     "lbm_encode_f64": ([_d, _vp, _vp, _i, _u64], _i),
     "lbm_decode_f64": ([_d, _vp, _i, _vp, _u64], _i),
+    "lbm_set_staged_config": ([_i, _i, _i, _i, _i], _i),
+    "lbm_get_staged_config": ([_i, _i, _vp, _vp, _vp], _i),
+    "lbm_device_error": ([_i], _i),
+    "lbm_selftest_wait_timeout": ([_d, _vp, _u64, _u64], _i),
 }
 
 
@@ -116,6 +121,24 @@ def check(code: int, what: str) -> None:
 def call(name: str, *args) -> None:  # noqa: ANN002
     """Call an int-returning entry point and raise LbmError on a non-zero status."""
     check(getattr(load(), name)(*args), name)
+
+
+def staged_config(lattice: int, elem_bytes: int) -> tuple[int, int, int]:
+    """(width, stages, warps) of the TMA-staged kernels."""
+    w, s, k = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    call("lbm_get_staged_config", lattice, elem_bytes, ctypes.byref(w), ctypes.byref(s),
+         ctypes.byref(k))
+    return w.value, s.value, k.value
+
+
+def set_staged_config(lattice: int, elem_bytes: int, width: int, stages: int,
+                      warps: int) -> None:
+    call("lbm_set_staged_config", lattice, elem_bytes, width, stages, warps)
+
+
+def device_error(clear: bool = True) -> int:
+    """0, or E_TIMEOUT when a kernel's bounded wait gave up (synchronises the device)."""
+    return load().lbm_device_error(int(clear))
 
 
 def lattice_info(lattice: int) -> dict:

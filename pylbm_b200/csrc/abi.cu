@@ -10,6 +10,19 @@
 
 using namespace lbm;
 
+namespace lbm {
+
+namespace {
+// [lattice][16-bit storage]: row-segment width, ring depth, consumer warps
+StagedTune g_tune[2][2] = {{{512, 4, 4}, {1024, 4, 4}}, {{256, 4, 4}, {512, 4, 4}}};
+}  // namespace
+
+StagedTune staged_tune(int lattice, int elem_bytes) {
+    return g_tune[lattice == LBM_D3Q19 ? 1 : 0][elem_bytes == 2 ? 1 : 0];
+}
+
+}  // namespace lbm
+
 namespace {
 
 bool finite(float v) { return std::isfinite(v); }
@@ -63,6 +76,46 @@ int check_pattern(const LbmDesc& d, const void* src, const void* dst, int patter
 extern "C" {
 
 int lbm_abi_version(void) { return LBM_ABI_VERSION; }
+
+int lbm_set_staged_config(int lattice, int elem_bytes, int width, int stages, int warps) {
+    if (lattice != LBM_D2Q9 && lattice != LBM_D3Q19) return LBM_E_LATTICE;
+    if (elem_bytes != 2 && elem_bytes != 4) return LBM_E_STORAGE;
+    if (width < 8 || width > 4096 || (width % 8) != 0) return LBM_E_ARG;
+    if (stages < 2 || stages > 8 || warps < 1 || warps > 8) return LBM_E_ARG;
+    const int q = q_of(lattice);
+    const long long smem = 128 + (long long)stages * q * (width + 2 * (16 / elem_bytes)) * elem_bytes;
+    if (smem > 227 * 1024) return LBM_E_SIZE;
+    g_tune[lattice == LBM_D3Q19 ? 1 : 0][elem_bytes == 2 ? 1 : 0] = {width, stages, warps};
+    return LBM_OK;
+}
+
+int lbm_get_staged_config(int lattice, int elem_bytes, int* width, int* stages, int* warps) {
+    if (lattice != LBM_D2Q9 && lattice != LBM_D3Q19) return LBM_E_LATTICE;
+    if (elem_bytes != 2 && elem_bytes != 4) return LBM_E_STORAGE;
+    if (!width || !stages || !warps) return LBM_E_NULL;
+    const StagedTune t = staged_tune(lattice, elem_bytes);
+    *width = t.width;
+    *stages = t.stages;
+    *warps = t.warps;
+    return LBM_OK;
+}
+
+int lbm_device_error(int clear) {
+    unsigned int bits = 0;
+    const int rc = read_device_error(clear, &bits);
+    if (rc) return rc;
+    return bits ? LBM_E_TIMEOUT : LBM_OK;
+}
+
+int lbm_selftest_wait_timeout(const LbmDesc* d, void* buf, uint64_t timeout_ns,
+                              uint64_t stream) {
+    int rc = lbm_validate(d);
+    if (rc) return rc;
+    if (d->lattice != LBM_D3Q19) return LBM_E_LATTICE;
+    if ((rc = check_buffer(*d, buf))) return rc;
+    if (timeout_ns == 0 || timeout_ns > 10000000000ull) return LBM_E_ARG;
+    return launch_staged_timeout_probe(*d, buf, timeout_ns, as_stream(stream));
+}
 
 const char* lbm_error_string(int code) {
     switch (code) {

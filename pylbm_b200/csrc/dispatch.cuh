@@ -33,6 +33,26 @@ int launch_fast_d2q9(const LbmDesc& d, const void* src, void* dst, int pattern,
 int launch_fast_d3q19(const LbmDesc& d, const void* src, void* dst, int pattern,
                       cudaStream_t s);
 
+// Per-launch configuration of the TMA-staged kernels (see lbm_set_staged_config).
+struct StagedTune {
+    int width;   // nodes per row segment
+    int stages;  // ring depth
+    int warps;   // consumer warps
+};
+
+// Process-wide tuning table (abi.cu), by lattice and bytes per stored element.
+StagedTune staged_tune(int lattice, int elem_bytes);
+
+// Device error word (errors.cu): its device address on the current device, and a read that
+// synchronises the device first.
+unsigned int* device_error_ptr();
+int read_device_error(int clear, unsigned int* bits);
+
+// Staged-kernel self test (step_d3q19.cu): a launch whose producer issues no copy, so every
+// consumer wait runs out after timeout_ns and records the timeout in the device error word.
+int launch_staged_timeout_probe(const LbmDesc& d, void* buf, unsigned long long timeout_ns,
+                                cudaStream_t s);
+
 // Helpers (helpers.cu)
 int launch_encode(const LbmDesc& d, const double* f64, void* buf, int layout, cudaStream_t s);
 int launch_decode(const LbmDesc& d, const void* buf, int layout, double* f64, cudaStream_t s);

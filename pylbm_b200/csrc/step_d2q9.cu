@@ -28,6 +28,7 @@
 #include "dispatch.cuh"
 #include "lattice.cuh"
 #include "params.cuh"
+#include "staged_launch.cuh"
 #include "vec.cuh"
 
 namespace lbm {
@@ -301,8 +302,13 @@ k_d2q9_aa_odd(const StepParams P, void* Av) {
 }
 
 template <int STORE, int COLL, bool FORCE>
-int go(const StepParams& P, const void* src, void* dst, int pattern, cudaStream_t s) {
+int go(const StepParams& P, const void* src, void* dst, int pattern, cudaStream_t s,
+       bool staged) {
     constexpr int V = VT<STORE>::V;
+    if (staged && pattern == LBM_PATTERN_AB)
+        return go_staged<L, STORE, COLL, FORCE, LBM_PATTERN_AB>(P, src, dst, s);
+    if (staged && pattern == LBM_PATTERN_AA_ODD)
+        return go_staged<L, STORE, COLL, FORCE, LBM_PATTERN_AA_ODD>(P, dst, dst, s);
     if (pattern == LBM_PATTERN_AA_EVEN) {
         const int threads = P.N / V;
         k_d2q9_aa_even<STORE, COLL, FORCE>
@@ -321,8 +327,9 @@ int go(const StepParams& P, const void* src, void* dst, int pattern, cudaStream_
 template <int STORE, int COLL>
 int go_f(const LbmDesc& d, const StepParams& P, const void* src, void* dst, int pattern,
          cudaStream_t s) {
-    return needs_force(d) ? go<STORE, COLL, true>(P, src, dst, pattern, s)
-                          : go<STORE, COLL, false>(P, src, dst, pattern, s);
+    const bool staged = (d.flags & LBM_FLAG_STAGED) != 0;
+    return needs_force(d) ? go<STORE, COLL, true>(P, src, dst, pattern, s, staged)
+                          : go<STORE, COLL, false>(P, src, dst, pattern, s, staged);
 }
 
 template <int STORE>
@@ -332,7 +339,9 @@ int go_c(const LbmDesc& d, const StepParams& P, const void* src, void* dst, int 
         case LBM_BGK: return go_f<STORE, LBM_BGK>(d, P, src, dst, pattern, s);
         case LBM_TRT: return go_f<STORE, LBM_TRT>(d, P, src, dst, pattern, s);
         case LBM_MRT: return go_f<STORE, LBM_MRT>(d, P, src, dst, pattern, s);
-        case LBM_STREAM_ONLY: return go<STORE, LBM_STREAM_ONLY, false>(P, src, dst, pattern, s);
+        case LBM_STREAM_ONLY:
+            return go<STORE, LBM_STREAM_ONLY, false>(P, src, dst, pattern, s,
+                                                     (d.flags & LBM_FLAG_STAGED) != 0);
     }
     return LBM_E_COLLISION;
 }

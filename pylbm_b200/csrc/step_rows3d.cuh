@@ -1,0 +1,195 @@
+// Vectorised D3Q19 register kernels: the D2Q9 row design (step_d2q9.cu) over rows (y, z).
+//
+// Every lane owns V consecutive nodes of one row (16 bytes per plane: 4 fp32 or 8 x 16-bit);
+// the 19 source row segments are read with aligned 16-byte loads at rows (y - c_iy, z - c_iz),
+// shifted along x in registers with one warp shuffle per x-moving plane, and the warp's two
+// halo elements are scalar loads. A block covers several rows when a row has fewer than 128
+// lanes (block (lanes_x, rows)), so 256-wide rows still fill whole warps; warps never straddle
+// rows. Rows next to a y or z wall take a general path with the wall and lid logic; all other
+// rows run without it (the branch is uniform per warp).
+#pragma once
+
+#include "codec.cuh"
+#include "collide.cuh"
+#include "lattice.cuh"
+#include "params.cuh"
+#include "vec.cuh"
+
+namespace lbm {
+namespace rows3d {
+
+using L = D3Q19;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kThreads = 128;
+
+// Source row (y - cy, z - cz), wrapped; EDGE rows report walls (then not wrapped) and top.
+template <bool EDGE>
+__device__ __forceinline__ int src_row(const StepParams& P, int y, int z, int cy, int cz,
+                                       bool& wall, bool& top) {
+    int ys = y - cy, zs = z - cz;
+    wall = top = false;
+    if constexpr (!EDGE) {
+        ys += ys < 0 ? P.n[1] : (ys >= P.n[1] ? -P.n[1] : 0);
+        zs += zs < 0 ? P.n[2] : (zs >= P.n[2] ? -P.n[2] : 0);
+    } else {
+        if (ys < 0 || ys >= P.n[1]) {
+            if (P.per[1]) ys += ys < 0 ? P.n[1] : -P.n[1];
+            else wall = true;
+        }
+        if (zs < 0 || zs >= P.n[2]) {
+            if (P.per[2]) zs += zs < 0 ? P.n[2] : -P.n[2];
+            else { wall = true; top = zs >= P.n[2]; }
+        }
+    }
+    return ys + P.n[1] * zs;
+}
+
+struct Lane3 {
+    int x0, y, z, lane;
+    bool active, first, last;
+};
+
+template <int V>
+__device__ __forceinline__ Lane3 lane_of(const StepParams& P) {
+    Lane3 l;
+    l.lane = threadIdx.x & 31;
+    l.x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+    l.y = blockIdx.y * blockDim.y + threadIdx.y;
+    l.z = blockIdx.z;
+    l.active = l.x0 < P.n[0] && l.y < P.n[1];
+    l.first = l.lane == 0;
+    l.last = l.active && (l.lane == 31 || l.x0 + V >= P.n[0]);
+    return l;
+}
+
+__device__ __forceinline__ bool edge_row(const StepParams& P, int y, int z) {
+    return (!P.per[1] && (y == 0 || y == P.n[1] - 1)) ||
+           (!P.per[2] && (z == 0 || z == P.n[2] - 1));
+}
+
+template <int STORE, bool READ_OPP, bool NC, bool EDGE>
+__device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT<STORE>::E* A,
+                                          const Lane3& l, uint4 (&v)[19], float (&lid)[19]) {
+    using E = typename VT<STORE>::E;
+    constexpr int V = VT<STORE>::V;
+    const int nx = P.n[0], N = P.N;
+    const int own_row = l.y + P.n[1] * l.z;
+    uint32_t halo[19];
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        const int cx = L::cx(i);
+        const int src_slot = READ_OPP ? L::opp(i) : i;
+        const int bb_slot = READ_OPP ? i : L::opp(i);
+        bool wall, top;
+        const int r = src_row<EDGE>(P, l.y, l.z, L::cy(i), L::cz(i), wall, top);
+        lid[i] = (wall && top && cx != 0) ? 6.0f * L::w(i) * float(cx) * P.ulid : 0.0f;
+        v[i] = make_uint4(0u, 0u, 0u, 0u);
+        halo[i] = 0u;
+        if (!l.active) continue;
+        if (wall) {
+            const E* p = A + bb_slot * N + own_row * nx + l.x0;
+            v[i] = NC ? ld_nc(p) : ld_plain(p);
+            continue;
+        }
+        const E* row = A + src_slot * N + r * nx;
+        v[i] = NC ? ld_nc(row + l.x0) : ld_plain(row + l.x0);
+        if (cx == 1 && l.first) {
+            const E* h = l.x0 > 0 ? row + l.x0 - 1
+                                  : (P.per[0] ? row + nx - 1 : A + bb_slot * N + own_row * nx);
+            halo[i] = NC ? ld1_nc(h) : ld1(h);
+        }
+        if (cx == -1 && l.last) {
+            const E* h = l.x0 + V < nx ? row + l.x0 + V
+                                       : (P.per[0] ? row : A + bb_slot * N + own_row * nx + nx - 1);
+            halo[i] = NC ? ld1_nc(h) : ld1(h);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        const int cx = L::cx(i);
+        if (cx == 0) continue;
+        bool wall, top;
+        src_row<EDGE>(P, l.y, l.z, L::cy(i), L::cz(i), wall, top);
+        if (cx == 1) {
+            uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
+            if (l.first) up = halo[i];
+            if (!wall) {
+#pragma unroll
+                for (int k = V - 1; k > 0; --k) put<V>(v[i], k, elem<V>(v[i], k - 1));
+                put<V>(v[i], 0, up);
+            }
+        } else {
+            uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
+            if (l.last) dn = halo[i];
+            if (!wall) {
+#pragma unroll
+                for (int k = 0; k < V - 1; ++k) put<V>(v[i], k, elem<V>(v[i], k + 1));
+                put<V>(v[i], V - 1, dn);
+            }
+        }
+    }
+}
+
+template <int STORE, int COLL, bool FORCE, bool LIDS>
+__device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19],
+                                             const float (&lid)[19]) {
+    using T = VT<STORE>;
+    constexpr int V = T::V;
+    const float F[3] = {P.F[0], P.F[1], P.F[2]};
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        float f[19];
+#pragma unroll
+        for (int i = 0; i < 19; ++i) {
+            f[i] = T::f(elem<V>(v[i], k));
+            if (LIDS) f[i] += lid[i];
+        }
+        collide<L, COLL, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+        for (int i = 0; i < 19; ++i) put<V>(v[i], k, T::b(f[i]));
+    }
+}
+
+template <int STORE, int COLL, bool FORCE, bool EDGE>
+__device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<STORE>::E* A,
+                                       typename VT<STORE>::E* B, const Lane3& l) {
+    uint4 v[19];
+    float lid[19];
+    pull_rows<STORE, false, true, EDGE>(P, A, l, v, lid);
+    if (!l.active) return;
+    collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid);
+    const int n0 = (l.y + P.n[1] * l.z) * P.n[0] + l.x0;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) st_cs(B + i * P.N + n0, v[i]);
+}
+
+template <int STORE, int COLL, bool FORCE>
+__global__ void __launch_bounds__(kThreads)
+k_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
+    using E = typename VT<STORE>::E;
+    const E* __restrict__ A = static_cast<const E*>(Av);
+    E* __restrict__ B = static_cast<E*>(Bv);
+    const Lane3 l = lane_of<VT<STORE>::V>(P);
+    if (edge_row(P, l.y, l.z)) ab_row<STORE, COLL, FORCE, true>(P, A, B, l);
+    else ab_row<STORE, COLL, FORCE, false>(P, A, B, l);
+}
+
+// Block shape (lanes along x, rows) for rows of nx nodes.
+inline dim3 block_for_rows(int nx, int V) {
+    int lanes = (nx / V + 31) / 32 * 32;
+    if (lanes > kThreads) lanes = kThreads;
+    return dim3(lanes, kThreads / lanes);
+}
+
+template <int STORE, int COLL, bool FORCE>
+int go_ab(const StepParams& P, const void* src, void* dst, cudaStream_t s) {
+    constexpr int V = VT<STORE>::V;
+    const dim3 block = block_for_rows(P.n[0], V);
+    const dim3 grid((P.n[0] / V + block.x - 1) / block.x, (P.n[1] + block.y - 1) / block.y,
+                    P.n[2]);
+    k_ab<STORE, COLL, FORCE><<<grid, block, 0, s>>>(P, src, dst);
+    return int(cudaGetLastError());
+}
+
+}  // namespace rows3d
+}  // namespace lbm

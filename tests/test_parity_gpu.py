@@ -333,3 +333,91 @@ def test_fast_lid_terms_match_oracle():
     case = O.Case(p.shape, p.tau, p.collision, p.periodic, p.u_lid, p.force)
     want = np.stack(O.stream(np.zeros(shp), case))
     np.testing.assert_allclose(out.cpu().numpy().reshape(shp), want, rtol=1e-6, atol=0)
+
+
+# ----------------------------------------------------------------------------- staged (TMA)
+STAGED_SHAPES = [((24, 5, 4), (True, True, True)), ((16, 6, 5), (False, False, False)),
+                 ((40, 3, 4), (True, False, True)), ((264, 2, 3), (False, True, False)),
+                 ((520, 3, 2), (True, True, True))]
+
+
+@pytest.mark.parametrize("storage", ["f32s", "f16"])
+@pytest.mark.parametrize("shape,per", STAGED_SHAPES)
+@pytest.mark.parametrize("aa", [False, True])
+def test_staged_d3q19_stream_permutation_bit_exact(storage, shape, per, aa):
+    test_fast_stream_permutation_bit_exact(storage, shape, per, aa)
+
+
+@pytest.mark.parametrize("storage", ["f32s", "bf16"])
+@pytest.mark.parametrize("shape,per", FAST_SHAPES[:3])
+@pytest.mark.parametrize("aa", [False, True])
+def test_staged_d2q9_stream_permutation_bit_exact(storage, shape, per, aa, monkeypatch):
+    from pylbm_b200 import _lib
+
+    orig = _stream_only
+
+    def staged(p, sid):
+        d = orig(p, sid)
+        d.flags = _lib.FLAG_STAGED
+        return d
+
+    monkeypatch.setitem(globals(), "_stream_only", staged)
+    test_fast_stream_permutation_bit_exact(storage, shape, per, aa)
+
+
+@pytest.mark.parametrize("variant", ["fused", "fused-aa", "fused-fp16"])
+def test_staged_d2q9_matches_register_kernel(variant):
+    from pylbm_b200 import _lib
+    from pylbm_b200.lattice import equilibrium
+    from pylbm_b200.problem import Problem
+
+    p = Problem((1032, 24), tau=0.6, u_lid=0.07, collision="trt")
+    rng = np.random.default_rng(8)
+    f0 = equilibrium(p.lattice, 1 + 0.01 * rng.standard_normal(p.array_shape),
+                     0.04 * (rng.random((2,) + p.array_shape) - 0.5))
+    a = _backend().VARIANTS[variant](p)
+    b = _backend().VARIANTS[variant](p)
+    b.desc.flags = _lib.FLAG_STAGED
+    for s in (a, b):
+        s.set_populations(f0)
+        s.step(30)
+    assert np.abs(a.populations() - b.populations()).max() < (1e-6 if a.storage == "f32" else 1e-3)
+
+
+@pytest.mark.parametrize("variant", ["fused", "fused-aa", "fused-bf16"])
+def test_staged_d3q19_matches_generic_kernel(variant):
+    from pylbm_b200 import _lib
+    from pylbm_b200 import workloads as W
+    from pylbm_b200.problem import Problem
+
+    p = Problem((40, 12, 10), tau=0.55, u_lid=0.05, collision="trt", periodic=(True, False, False))
+    f0 = W.taylor_green_3d_populations(40)[:, :10, :12, :]
+    a = _backend().VARIANTS[variant](p)
+    g = _backend().VARIANTS[variant](p)
+    g.desc.flags = _lib.FLAG_GENERIC
+    for s in (a, g):
+        s.set_populations(f0)
+        s.step(20)
+    assert np.abs(a.populations() - g.populations()).max() < (1e-6 if a.storage == "f32" else 1e-3)
+
+
+def test_bounded_wait_reports_timeout_and_context_survives():
+    """Failure detection without a fault: a staged launch whose producer issues nothing makes
+    every consumer wait run out; the device error word reports it, the context stays usable."""
+    from pylbm_b200 import _lib
+    from pylbm_b200.backend import make_desc
+    from pylbm_b200.problem import Problem
+
+    p = Problem((32, 8, 8), periodic=(True, True, True), collision="trt")
+    d = make_desc(p, _lib.STORE_F32_SHIFTED)
+    buf = torch.zeros(19 * p.n_nodes, dtype=torch.float32, device="cuda")
+    assert _lib.device_error(clear=True) == 0
+    _lib.call("lbm_selftest_wait_timeout", ctypes.byref(d), buf.data_ptr(), 20_000_000, 0)
+    assert _lib.device_error(clear=True) == _lib.E_TIMEOUT
+    assert _lib.device_error(clear=True) == 0
+    assert torch.count_nonzero(buf).item() == 0
+    s = _backend().B200Fused(p)
+    s.step(4)
+    s.synchronize()
+    assert _lib.device_error(clear=False) == 0
+    assert np.isfinite(s.populations()).all()
