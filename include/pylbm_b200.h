@@ -127,6 +127,16 @@ int lbm_advance(const LbmDesc* d, void* a, void* b, int aa, int nsteps, uint64_t
 int lbm_moments_f64(const LbmDesc* d, const void* f, int layout, double* out,
                     uint64_t stream);
 
+/* The same sums without allocating: for callers that cannot let a library allocate device
+ * memory (an application whose own pool owns all of it, or a loop that must not risk an
+ * allocation stall or failure mid-run). No counterpart in pylbm. The partial sums live in a
+ * fixed 75,776-byte array in the library's device image (2368 rows; larger needs are refused
+ * with LBM_E_SIZE), one copy per device until exit. The first call on a device looks up that
+ * array's address and should come before any stream capture. All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+int lbm_moments_f64_noalloc(const LbmDesc* d, const void* f, int layout, double* out,
+                            uint64_t stream);
+
 /* Device macroscopic fields from a stored state: rho[N], u[d * N] (fp32), with the physical
  * velocity u = (sum c f - F/2) / rho of pylbm's core.macroscopic (core.py:255-266). */
 int lbm_macroscopic(const LbmDesc* d, const void* f, int layout, float* rho, float* u,

@@ -69,6 +69,7 @@ _SIGNATURES = {
     "lbm_launch": ([_d, _vp, _vp, _i, _u64], _i),
     "lbm_advance": ([_d, _vp, _vp, _i, _i, _u64], _i),
     "lbm_moments_f64": ([_d, _vp, _i, _vp, _u64], _i),
+    "lbm_moments_f64_noalloc": ([_d, _vp, _i, _vp, _u64], _i),
     "lbm_macroscopic": ([_d, _vp, _i, _vp, _vp, _u64], _i),
     "lbm_encode_f64": ([_d, _vp, _vp, _i, _u64], _i),
     "lbm_decode_f64": ([_d, _vp, _i, _vp, _u64], _i),

@@ -59,5 +59,10 @@ int launch_decode(const LbmDesc& d, const void* buf, int layout, double* f64, cu
 int launch_macroscopic(const LbmDesc& d, const void* f, int layout, float* rho, float* u,
                        cudaStream_t s);
 int launch_moments(const LbmDesc& d, const void* f, int layout, double* out, cudaStream_t s);
+// Rows of partial sums the moment reduction uses for N nodes, and the reduction into
+// caller-provided scratch of 4 * rows doubles.
+int moments_rows(int N);
+int launch_moments_into(const LbmDesc& d, const void* f, int layout, double* out,
+                        double* scratch, int rows, cudaStream_t s);
 
 }  // namespace lbm

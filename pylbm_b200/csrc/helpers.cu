@@ -217,6 +217,15 @@ int launch_macroscopic(const LbmDesc& d, const void* f, int layout, float* rho, 
     });
 }
 
+int moments_rows(int N) { return grid_for(N); }
+
+// The two moment passes with caller-provided scratch of at least 4 * rows doubles.
+int launch_moments_into(const LbmDesc& d, const void* f, int layout, double* out,
+                        double* scratch, int rows, cudaStream_t s) {
+    return d.lattice == LBM_D2Q9 ? moments_storage<D2Q9>(d, f, layout, out, scratch, rows, s)
+                                 : moments_storage<D3Q19>(d, f, layout, out, scratch, rows, s);
+}
+
 // The partial rows live in stream-ordered scratch from cudaMallocAsync, released on the
 // same stream after pass 2 has consumed them.
 int launch_moments(const LbmDesc& d, const void* f, int layout, double* out, cudaStream_t s) {
