@@ -24,14 +24,199 @@
 
 namespace lbm {
 
+// Shifted BGK / TRT on opposite pairs (i, o = opp(i), c_o = -c_i, w_o = w_i). With the pair
+// sums a = h_i + h_o and differences d = h_i - h_o: drho = h_0 + sum a, j = sum_pairs c_i d,
+// and the equilibrium splits into a symmetric part ep = w (drho + rho (4.5 (c.u)^2 - 1.5 u.u))
+// and an antisymmetric part em = 3 w rho c.u (heq_i = ep + em, heq_o = ep - em); the Guo
+// source likewise into S+ = w (9 (c.u)(c.F) - 3 u.F) and S- = 3 w c.F. TRT relaxes the two
+// parts with s+ = r0 and s- = r1 directly; BGK relaxes heq_i, heq_o with r0. Same algebra as
+// the per-direction form with about a third fewer instructions: the 16-bit kernels, whose
+// bandwidth needs twice the node rate of fp32, are bound by instruction issue, not HBM.
+template <class L, int COLL, bool FORCE>
+__device__ __forceinline__ void collide_pairs(float (&h)[L::Q], const float (&F)[3], float r0,
+                                              float r1) {
+    constexpr int Q = L::Q;
+    constexpr int D = L::D;
+    float a[Q], d[Q];
+    float drho = h[0];
+#pragma unroll
+    for (int i = 1; i < Q; ++i) {
+        const int o = L::opp(i);
+        if (o < i) continue;
+        a[i] = h[i] + h[o];
+        d[i] = h[i] - h[o];
+        drho += a[i];
+    }
+    float j[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int ax = 0; ax < D; ++ax) {
+        bool started = false;
+#pragma unroll
+        for (int i = 1; i < Q; ++i) {
+            if (L::opp(i) < i) continue;
+            const int c = cc<L>(i, ax);
+            if (c == 0) continue;
+            if (!started) {
+                j[ax] = c > 0 ? d[i] : -d[i];
+                started = true;
+            } else {
+                j[ax] = c > 0 ? j[ax] + d[i] : j[ax] - d[i];
+            }
+        }
+    }
+    const float rho = 1.0f + drho;
+    const float inv_rho = 1.0f / rho;
+    float u[3];
+#pragma unroll
+    for (int ax = 0; ax < D; ++ax) u[ax] = (FORCE ? j[ax] + 0.5f * F[ax] : j[ax]) * inv_rho;
+    float usq = u[0] * u[0];
+#pragma unroll
+    for (int ax = 1; ax < D; ++ax) usq += u[ax] * u[ax];
+    const float t = -1.5f * usq;
+    float uf = 0.0f;
+    if (FORCE) {
+        uf = u[0] * F[0];
+#pragma unroll
+        for (int ax = 1; ax < D; ++ax) uf += u[ax] * F[ax];
+    }
+    const float gp = 1.0f - 0.5f * r0;
+    const float gm = 1.0f - 0.5f * (COLL == LBM_TRT ? r1 : r0);
+    {  // rest population
+        const float w0 = L::w(0);
+        const float heq = w0 * drho + (w0 * rho) * t;
+        float p = h[0] + r0 * (heq - h[0]);
+        if (FORCE) p += gp * (w0 * (-3.0f * uf));
+        h[0] = p;
+    }
+#pragma unroll
+    for (int i = 1; i < Q; ++i) {
+        const int o = L::opp(i);
+        if (o < i) continue;
+        const float w = L::w(i);
+        float cu = 0.0f, cf = 0.0f;
+#pragma unroll
+        for (int ax = 0; ax < D; ++ax) {
+            const int c = cc<L>(i, ax);
+            if (c == 1) {
+                cu += u[ax];
+                if (FORCE) cf += F[ax];
+            }
+            if (c == -1) {
+                cu -= u[ax];
+                if (FORCE) cf -= F[ax];
+            }
+        }
+        const float ep = (w * drho) + (w * rho) * fmaf(4.5f * cu, cu, t);
+        const float em = (3.0f * w * rho) * cu;
+        float sp = 0.0f, sm = 0.0f;
+        if (FORCE) {
+            sp = w * (9.0f * cu * cf - 3.0f * uf);
+            sm = 3.0f * w * cf;
+        }
+        float pi, po;
+        if (COLL == LBM_TRT) {
+            const float np_ = 0.5f * a[i] - ep;
+            const float nm_ = 0.5f * d[i] - em;
+            pi = h[i] - r0 * np_ - r1 * nm_;
+            po = h[o] - r0 * np_ + r1 * nm_;
+            if (FORCE) {
+                pi += gp * sp + gm * sm;
+                po += gp * sp - gm * sm;
+            }
+        } else {
+            pi = h[i] + r0 * ((ep + em) - h[i]);
+            po = h[o] + r0 * ((ep - em) - h[o]);
+            if (FORCE) {
+                pi += gp * (sp + sm);
+                po += gp * (sp - sm);
+            }
+        }
+        h[i] = pi;
+        h[o] = po;
+    }
+}
+
+// Shifted D2Q9 MRT in moment space. Moments of h (= M f - M w, M w = (1, -2, 1, 0, ...)) from
+// shared partial sums; equilibrium moments of the second-order feq in closed form,
+// e = -2 drho + 3 rho u.u, eps = drho - 3 rho u.u, q = -rho u, pxx = rho (ux^2 - uy^2),
+// pxy = rho ux uy; Guo source moments M S = (0, 6 u.F, -6 u.F, Fx, -Fx, Fy, -Fy,
+// 2 (ux Fx - uy Fy), ux Fy + uy Fx); then h* = h + M^T (dm / |M_k|^2). Algebraically the
+// update of lattice.py:71-109 / core.py:228-246 with rates (0, r1, r2, 0, r3, 0, r3, r0, r0).
+template <bool FORCE>
+__device__ __forceinline__ void collide_mrt_moments(float (&h)[9], const float (&F)[3],
+                                                    float r0, float r1, float r2, float r3) {
+    const float ax_ = (h[1] + h[3]) + (h[2] + h[4]);
+    const float dg_ = (h[5] + h[7]) + (h[6] + h[8]);
+    const float drho = h[0] + ax_ + dg_;
+    const float m_e = -4.0f * h[0] - ax_ + 2.0f * dg_;
+    const float m_eps = 4.0f * h[0] - 2.0f * ax_ + dg_;
+    const float dx = h[1] - h[3], dy = h[2] - h[4];
+    const float p57 = h[5] - h[7], p86 = h[8] - h[6];
+    const float jx = dx + (p57 + p86), jy = dy + (p57 - p86);
+    const float m_qx = -2.0f * dx + (p57 + p86);
+    const float m_qy = -2.0f * dy + (p57 - p86);
+    const float m_pxx = (h[1] + h[3]) - (h[2] + h[4]);
+    const float m_pxy = (h[5] + h[7]) - (h[6] + h[8]);
+    const float rho = 1.0f + drho;
+    const float inv_rho = 1.0f / rho;
+    const float ux = (FORCE ? jx + 0.5f * F[0] : jx) * inv_rho;
+    const float uy = (FORCE ? jy + 0.5f * F[1] : jy) * inv_rho;
+    const float usq3 = 3.0f * rho * (ux * ux + uy * uy);
+    float de = -r1 * (m_e - (-2.0f * drho + usq3));
+    float deps = -r2 * (m_eps - (drho - usq3));
+    float dqx = -r3 * (m_qx + rho * ux);
+    float dqy = -r3 * (m_qy + rho * uy);
+    float dpxx = -r0 * (m_pxx - rho * (ux * ux - uy * uy));
+    float dpxy = -r0 * (m_pxy - rho * ux * uy);
+    float djx = 0.0f, djy = 0.0f;
+    if (FORCE) {
+        const float uf = ux * F[0] + uy * F[1];
+        de += (1.0f - 0.5f * r1) * (6.0f * uf);
+        deps += (1.0f - 0.5f * r2) * (-6.0f * uf);
+        dqx += (1.0f - 0.5f * r3) * (-F[0]);
+        dqy += (1.0f - 0.5f * r3) * (-F[1]);
+        dpxx += (1.0f - 0.5f * r0) * (2.0f * (ux * F[0] - uy * F[1]));
+        dpxy += (1.0f - 0.5f * r0) * (ux * F[1] + uy * F[0]);
+        djx = F[0];
+        djy = F[1];
+    }
+    // back-transform with the squared row norms (9, 36, 36, 6, 12, 6, 12, 4, 4)
+    const float ne = de * (1.0f / 36.0f), neps = deps * (1.0f / 36.0f);
+    const float njx = djx * (1.0f / 6.0f), njy = djy * (1.0f / 6.0f);
+    const float nqx = dqx * (1.0f / 12.0f), nqy = dqy * (1.0f / 12.0f);
+    const float npxx = dpxx * 0.25f, npxy = dpxy * 0.25f;
+    const float A = -ne - 2.0f * neps;
+    const float Bd = 2.0f * ne + neps;
+    const float X = njx - 2.0f * nqx, Y = njy - 2.0f * nqy;
+    const float Xd = njx + nqx, Yd = njy + nqy;
+    h[0] += -4.0f * ne + 4.0f * neps;
+    h[1] += A + X + npxx;
+    h[3] += A - X + npxx;
+    h[2] += A + Y - npxx;
+    h[4] += A - Y - npxx;
+    h[5] += Bd + Xd + Yd + npxy;
+    h[6] += Bd - Xd + Yd - npxy;
+    h[7] += Bd - Xd - Yd + npxy;
+    h[8] += Bd + Xd - Yd - npxy;
+}
+
 // In: f[] pre-collision (h if SHIFT), F = total force at the node (zeros when unforced).
-// Out: f[] post-collision (h* if SHIFT).
+// Out: f[] post-collision (h* if SHIFT). Shifted storages use the pair / moment-space forms
+// above; the plain form below keeps pylbm's per-direction order (lbm.cu:100-163).
 template <class L, int COLL, bool SHIFT, bool FORCE>
 __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], float r0,
                                         float r1, float r2, float r3) {
     constexpr int Q = L::Q;
     constexpr int D = L::D;
     if constexpr (COLL == LBM_STREAM_ONLY) return;  // debug mode: streaming only
+    if constexpr (SHIFT && (COLL == LBM_BGK || COLL == LBM_TRT)) {
+        collide_pairs<L, COLL, FORCE>(f, F, r0, r1);
+        return;
+    }
+    if constexpr (SHIFT && COLL == LBM_MRT && Q == 9) {
+        collide_mrt_moments<FORCE>(f, F, r0, r1, r2, r3);
+        return;
+    }
     // ---------------------------------------------------------------- moments
     float rho_s = 0.0f;  // rho (plain) or drho (shifted)
 #pragma unroll

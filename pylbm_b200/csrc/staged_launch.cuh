@@ -73,14 +73,31 @@ __global__ void __launch_bounds__(128) k_aa_even(const StepParams P, void* Av) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) v[i] = ld_plain(A + i * P.N + n0);
     const float F[3] = {P.F[0], P.F[1], P.F[2]};
+    if constexpr (V == 4) {
 #pragma unroll
-    for (int k = 0; k < V; ++k) {
-        float f[Q];
+        for (int k = 0; k < V; ++k) {
+            float f[Q];
 #pragma unroll
-        for (int i = 0; i < Q; ++i) f[i] = T::f(elem<V>(v[i], k));
-        collide<L, COLL, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+            for (int i = 0; i < Q; ++i) f[i] = T::f(elem<V>(v[i], k));
+            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
-        for (int i = 0; i < Q; ++i) put<V>(v[i], k, T::b(f[i]));
+            for (int i = 0; i < Q; ++i) put<V>(v[i], k, T::b(f[i]));
+        }
+    } else {  // 16-bit: two nodes per word, packed conversions
+#pragma unroll
+        for (int jw = 0; jw < 4; ++jw) {
+            float f0[Q], f1[Q];
+#pragma unroll
+            for (int i = 0; i < Q; ++i) {
+                const float2 p = unpack2<STORE>(word(v[i], jw));
+                f0[i] = p.x;
+                f1[i] = p.y;
+            }
+            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f0, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f1, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+            for (int i = 0; i < Q; ++i) set_word(v[i], jw, pack2<STORE>(f0[i], f1[i]));
+        }
     }
 #pragma unroll
     for (int i = 0; i < Q; ++i) st_cs(A + L::opp(i) * P.N + n0, v[i]);

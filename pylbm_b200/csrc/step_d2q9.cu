@@ -113,19 +113,11 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
         if (cx == 1) {
             uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
             if (first) up = halo[i];
-            if (!wall) {
-#pragma unroll
-                for (int k = V - 1; k > 0; --k) put<V>(v[i], k, elem<V>(v[i], k - 1));
-                put<V>(v[i], 0, up);
-            }
+            if (!wall) v[i] = shift_up<V>(v[i], up);
         } else {
             uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
             if (last) dn = halo[i];
-            if (!wall) {
-#pragma unroll
-                for (int k = 0; k < V - 1; ++k) put<V>(v[i], k, elem<V>(v[i], k + 1));
-                put<V>(v[i], V - 1, dn);
-            }
+            if (!wall) v[i] = shift_down<V>(v[i], dn);
         }
     }
 }
@@ -140,17 +132,36 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[9],
     constexpr int V = T::V;
     constexpr bool SHIFT = Codec<STORE>::shifted;
     const float F[3] = {P.F[0], P.F[1], 0.0f};
+    if constexpr (V == 4) {
 #pragma unroll
-    for (int k = 0; k < V; ++k) {
-        float f[9];
+        for (int k = 0; k < V; ++k) {
+            float f[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            f[i] = T::f(elem<V>(v[i], k));
-            if (LIDS) f[i] += lid[i];
+            for (int i = 0; i < 9; ++i) {
+                f[i] = T::f(elem<V>(v[i], k));
+                if (LIDS) f[i] += lid[i];
+            }
+            collide<L, COLL, SHIFT, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) put<V>(v[i], k, T::b(LIDS ? f[i] - sub[i] : f[i]));
         }
-        collide<L, COLL, SHIFT, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+    } else {  // 16-bit: two nodes per word, packed conversions
 #pragma unroll
-        for (int i = 0; i < 9; ++i) put<V>(v[i], k, T::b(LIDS ? f[i] - sub[i] : f[i]));
+        for (int jw = 0; jw < 4; ++jw) {
+            float f0[9], f1[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                const float2 p = unpack2<STORE>(word(v[i], jw));
+                f0[i] = LIDS ? p.x + lid[i] : p.x;
+                f1[i] = LIDS ? p.y + lid[i] : p.y;
+            }
+            collide<L, COLL, SHIFT, FORCE>(f0, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, SHIFT, FORCE>(f1, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                set_word(v[i], jw, LIDS ? pack2<STORE>(f0[i] - sub[i], f1[i] - sub[i])
+                                        : pack2<STORE>(f0[i], f1[i]));
+        }
     }
 }
 
@@ -256,11 +267,7 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
             const uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
             if (!l.active) continue;
             if (!l.first) {
-                uint4 w;
-                put<V>(w, 0, up);
-#pragma unroll
-                for (int k = 1; k < V; ++k) put<V>(w, k, elem<V>(v[i], k - 1));
-                st_plain(plane + l.x0, w);
+                st_plain(plane + l.x0, shift_up<V>(v[i], up));
             } else {
 #pragma unroll
                 for (int k = 0; k < V - 1; ++k) st1(plane + l.x0 + 1 + k, elem<V>(v[i], k));
@@ -274,11 +281,7 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
             const uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
             if (!l.active) continue;
             if (!l.last) {
-                uint4 w;
-#pragma unroll
-                for (int k = 0; k < V - 1; ++k) put<V>(w, k, elem<V>(v[i], k + 1));
-                put<V>(w, V - 1, dn);
-                st_plain(plane + l.x0, w);
+                st_plain(plane + l.x0, shift_down<V>(v[i], dn));
             } else {
 #pragma unroll
                 for (int k = 1; k < V; ++k) st1(plane + l.x0 + k - 1, elem<V>(v[i], k));

@@ -113,19 +113,11 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
         if (cx == 1) {
             uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
             if (l.first) up = halo[i];
-            if (!wall) {
-#pragma unroll
-                for (int k = V - 1; k > 0; --k) put<V>(v[i], k, elem<V>(v[i], k - 1));
-                put<V>(v[i], 0, up);
-            }
+            if (!wall) v[i] = shift_up<V>(v[i], up);
         } else {
             uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
             if (l.last) dn = halo[i];
-            if (!wall) {
-#pragma unroll
-                for (int k = 0; k < V - 1; ++k) put<V>(v[i], k, elem<V>(v[i], k + 1));
-                put<V>(v[i], V - 1, dn);
-            }
+            if (!wall) v[i] = shift_down<V>(v[i], dn);
         }
     }
 }
@@ -136,17 +128,34 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19]
     using T = VT<STORE>;
     constexpr int V = T::V;
     const float F[3] = {P.F[0], P.F[1], P.F[2]};
+    if constexpr (V == 4) {
 #pragma unroll
-    for (int k = 0; k < V; ++k) {
-        float f[19];
+        for (int k = 0; k < V; ++k) {
+            float f[19];
 #pragma unroll
-        for (int i = 0; i < 19; ++i) {
-            f[i] = T::f(elem<V>(v[i], k));
-            if (LIDS) f[i] += lid[i];
+            for (int i = 0; i < 19; ++i) {
+                f[i] = T::f(elem<V>(v[i], k));
+                if (LIDS) f[i] += lid[i];
+            }
+            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+            for (int i = 0; i < 19; ++i) put<V>(v[i], k, T::b(f[i]));
         }
-        collide<L, COLL, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+    } else {  // 16-bit: two nodes per word, packed conversions
 #pragma unroll
-        for (int i = 0; i < 19; ++i) put<V>(v[i], k, T::b(f[i]));
+        for (int jw = 0; jw < 4; ++jw) {
+            float f0[19], f1[19];
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                const float2 p = unpack2<STORE>(word(v[i], jw));
+                f0[i] = LIDS ? p.x + lid[i] : p.x;
+                f1[i] = LIDS ? p.y + lid[i] : p.y;
+            }
+            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f0, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f1, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+            for (int i = 0; i < 19; ++i) set_word(v[i], jw, pack2<STORE>(f0[i], f1[i]));
+        }
     }
 }
 

@@ -9,6 +9,7 @@
 #include <cuda_fp16.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "../../include/pylbm_b200.h"
 
@@ -73,6 +74,53 @@ __device__ __forceinline__ void put(uint4& v, int k, uint32_t e) {
         const uint32_t w = word(v, k >> 1);
         set_word(v, k >> 1, (k & 1) ? ((w & 0x0000ffffu) | (e << 16)) : ((w & 0xffff0000u) | e));
     }
+}
+
+// Shift a vector by one element along x: shift_up gives element k = v[k - 1] and element 0 =
+// `up`; shift_down gives element k = v[k + 1] and element V - 1 = `dn` (the new elements sit
+// in the low bits of up / dn). For 16-bit elements each output word is one byte permutation
+// of two input words.
+template <int V>
+__device__ __forceinline__ uint4 shift_up(const uint4& v, uint32_t up) {
+    if constexpr (V == 4) {
+        return make_uint4(up, v.x, v.y, v.z);
+    } else {
+        return make_uint4(__byte_perm(up, v.x, 0x5410), __byte_perm(v.x, v.y, 0x5432),
+                          __byte_perm(v.y, v.z, 0x5432), __byte_perm(v.z, v.w, 0x5432));
+    }
+}
+template <int V>
+__device__ __forceinline__ uint4 shift_down(const uint4& v, uint32_t dn) {
+    if constexpr (V == 4) {
+        return make_uint4(v.y, v.z, v.w, dn);
+    } else {
+        return make_uint4(__byte_perm(v.x, v.y, 0x5432), __byte_perm(v.y, v.z, 0x5432),
+                          __byte_perm(v.z, v.w, 0x5432), __byte_perm(v.w, dn, 0x5432));
+    }
+}
+
+// Two 16-bit elements of one word <-> two floats (packed conversions).
+template <int STORE>
+__device__ __forceinline__ float2 unpack2(uint32_t w) {
+    if constexpr (STORE == LBM_STORE_F16) {
+        __half2 h;
+        memcpy(&h, &w, 4);
+        return __half22float2(h);
+    } else {
+        return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+    }
+}
+template <int STORE>
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+    uint32_t w;
+    if constexpr (STORE == LBM_STORE_F16) {
+        const __half2 h = __floats2half2_rn(lo, hi);
+        memcpy(&w, &h, 4);
+    } else {
+        const __nv_bfloat162 b = __floats2bfloat162_rn(lo, hi);
+        memcpy(&w, &b, 4);
+    }
+    return w;
 }
 
 // Whole-vector moves.
