@@ -52,7 +52,16 @@ WORKLOADS = {
     "d3q19-trt-ab-f16": ("D3Q19", 256, "trt", 0.55, "fused-fp16"),
     "d3q19-trt-ab-bf16": ("D3Q19", 256, "trt", 0.55, "fused-bf16"),
     "d3q19-trt-aa-f32": ("D3Q19", 256, "trt", 0.55, "fused-aa"),
+    # lid-driven cavities (walls on every axis, lid U = 0.05 on the top of the last axis)
+    "d2q9-bgk-cavity-f32": ("D2Q9", 4096, "bgk", 0.6, "fused"),
+    "d2q9-mrt-cavity-f32": ("D2Q9", 4096, "mrt", 0.6, "fused"),
+    "d2q9-mrt-cavity-f16": ("D2Q9", 4096, "mrt", 0.6, "fused-fp16"),
+    "d3q19-bgk-cavity-f32": ("D3Q19", 256, "bgk", 0.6, "fused"),
 }
+
+
+def is_cavity(name: str) -> bool:
+    return "cavity" in name
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -82,9 +91,10 @@ def make_problem(name: str, n: int | None = None):
 
     lat, n0, coll, tau, _ = WORKLOADS[name]
     n = n or n0
-    if lat == "D2Q9":
-        return Problem((n, n), tau=tau, collision=coll, periodic=(True, True))
-    return Problem((n, n, n), tau=tau, collision=coll, periodic=(True, True, True))
+    shape = (n, n) if lat == "D2Q9" else (n, n, n)
+    if is_cavity(name):
+        return Problem(shape, tau=tau, collision=coll, u_lid=0.05)
+    return Problem(shape, tau=tau, collision=coll, periodic=(True,) * len(shape))
 
 
 def initial_state(name: str, seed: int, n: int | None = None) -> np.ndarray:
@@ -92,6 +102,8 @@ def initial_state(name: str, seed: int, n: int | None = None) -> np.ndarray:
 
     lat, n0, *_ = WORKLOADS[name]
     n = n or n0
+    if is_cavity(name):  # fluid at rest, set in motion by the lid
+        return make_problem(name, n).initial_populations()
     if lat == "D2Q9":
         return W.fourier_populations(n, seed)
     return W.taylor_green_3d_populations(n)
@@ -158,7 +170,12 @@ def _oracle_band_worker(args: tuple) -> float:
     from pylbm_b200.lattice import D2Q9, D3Q19, equilibrium
 
     lat, n, coll, tau, _ = WORKLOADS[name]
-    if lat == "D2Q9":
+    if is_cavity(name):  # a cavity of the band's size: walls everywhere, lid on top
+        shape = (n, rows) if lat == "D2Q9" else (n, n, rows)
+        case = O.Case(shape, tau, coll, (False,) * len(shape), u_lid=0.05)
+        lattice = D2Q9 if lat == "D2Q9" else D3Q19
+        f = equilibrium(lattice, np.ones(shape[::-1]), np.zeros((len(shape),) + shape[::-1]))
+    elif lat == "D2Q9":
         rho, u = W.fourier_state(n, seed)
         f = equilibrium(D2Q9, rho[:rows], u[:, :rows])
         case = O.Case((n, rows), tau, coll, (True, True))
@@ -230,10 +247,15 @@ def config_of(name: str, a: argparse.Namespace) -> dict:
     lat, n, coll, tau, variant = WORKLOADS[name]
     n = a.n or n
     shape = [n, n] if lat == "D2Q9" else [n, n, n]
+    if is_cavity(name):
+        init = "lid-driven cavity, walls on every axis, lid U=0.05, fluid at rest"
+    elif lat == "D2Q9":
+        init = "rho=1+0.01N(0,1), u=8 seeded Fourier modes, max|u|=0.05"
+    else:
+        init = "Taylor-Green vortex u0=0.05, rho=1"
     return {"workload": name, "lattice": lat, "shape": shape, "collision": coll, "tau": tau,
-            "variant": variant, "periodic": True, "lbm_steps_per_step": a.lbm_steps,
-            "init": ("rho=1+0.01N(0,1), u=8 seeded Fourier modes, max|u|=0.05"
-                     if lat == "D2Q9" else "Taylor-Green vortex u0=0.05, rho=1"),
+            "variant": variant, "periodic": not is_cavity(name),
+            "lbm_steps_per_step": a.lbm_steps, "init": init,
             "l2": "state larger than L2 (no flush needed)", "parallelism": f"replicas x{a.gpus}"}
 
 

@@ -150,6 +150,25 @@ int lbm_encode_f64(const LbmDesc* d, const double* f64, void* buf, int layout,
 int lbm_decode_f64(const LbmDesc* d, const void* buf, int layout, double* f64,
                    uint64_t stream);
 
+/* Batches of independent D2Q9 lattices of uneven sizes (no pylbm counterpart: pylbm steps
+ * one lattice per solver). All lattices share collision and storage; each has its own shape,
+ * walls, lid speed and rates; nx must be a multiple of the 16-byte vector (4 fp32 / 8 x
+ * 16-bit). Lattice l occupies elements [offset_l, offset_l + 9 nx_l ny_l) of the two caller
+ * buffers, in the order given. One kernel launch advances every lattice by one step. */
+typedef struct LbmBatch LbmBatch;
+int lbm_batch_create(const LbmDesc* lattices, int count, LbmBatch** out);
+int lbm_batch_destroy(LbmBatch* b);
+int lbm_batch_info(const LbmBatch* b, int64_t* elements, int64_t* nodes, int* items);
+int lbm_batch_offsets(const LbmBatch* b, int64_t* offsets);
+/* launch shape, chosen by the autotuner: threads per block (64/128/256), blocks per SM */
+int lbm_batch_set_launch(LbmBatch* b, int block, int blocks_per_sm);
+int lbm_batch_get_launch(const LbmBatch* b, int* block, int* blocks_per_sm);
+/* nsteps pull steps, ping-pong a -> b -> a ...: the result is in a when nsteps is even */
+int lbm_batch_step(LbmBatch* b, void* a, void* bb, int nsteps, uint64_t stream);
+/* the same nsteps launches replayed from one CUDA graph, captured on first use for these
+ * buffers, step count and launch shape, and cached in the batch */
+int lbm_batch_graph_launch(LbmBatch* b, void* a, void* bb, int nsteps, uint64_t stream);
+
 /* Tuning of the TMA-staged kernels (D3Q19 always; D2Q9 with LBM_FLAG_STAGED), per lattice and
  * stored element size (2 or 4 bytes), process-wide: nodes per row segment (multiple of 8),
  * shared-memory ring depth (2..8) and consumer warps (1..8). No pylbm counterpart (pylbm

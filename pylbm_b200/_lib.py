@@ -73,6 +73,14 @@ _SIGNATURES = {
     "lbm_macroscopic": ([_d, _vp, _i, _vp, _vp, _u64], _i),
     "lbm_encode_f64": ([_d, _vp, _vp, _i, _u64], _i),
     "lbm_decode_f64": ([_d, _vp, _i, _vp, _u64], _i),
+    "lbm_batch_create": ([_d, _i, _vp], _i),
+    "lbm_batch_destroy": ([_vp], _i),
+    "lbm_batch_info": ([_vp, _vp, _vp, _vp], _i),
+    "lbm_batch_offsets": ([_vp, _vp], _i),
+    "lbm_batch_set_launch": ([_vp, _i, _i], _i),
+    "lbm_batch_get_launch": ([_vp, _vp, _vp], _i),
+    "lbm_batch_step": ([_vp, _vp, _vp, _i, _u64], _i),
+    "lbm_batch_graph_launch": ([_vp, _vp, _vp, _i, _u64], _i),
     "lbm_set_staged_config": ([_i, _i, _i, _i, _i], _i),
     "lbm_get_staged_config": ([_i, _i, _vp, _vp, _vp], _i),
     "lbm_device_error": ([_i], _i),

@@ -33,6 +33,21 @@ int launch_fast_d2q9(const LbmDesc& d, const void* src, void* dst, int pattern,
 int launch_fast_d3q19(const LbmDesc& d, const void* src, void* dst, int pattern,
                       cudaStream_t s);
 
+// One lattice of a batch (device table entry, batched.cu / step_d2q9.cu).
+struct BatchLattice {
+    long long base;     // element offset of the lattice's plane 0 in the batch buffers
+    int nx, ny;
+    int periodic_mask;
+    int item0;          // first warp work item of the lattice
+    int segs;           // warp segments (32 lanes x V nodes) per row
+    float ulid, r0, r1, r2, r3;
+};
+
+// One step of every lattice of a batch (D2Q9 pull, two buffers).
+int launch_batch_d2q9(int collision, int storage, const BatchLattice* lats, int nlat,
+                      int items, const void* src, void* dst, int grid, int block,
+                      cudaStream_t s);
+
 // Per-launch configuration of the TMA-staged kernels (see lbm_set_staged_config).
 struct StagedTune {
     int width;   // nodes per row segment

@@ -351,7 +351,101 @@ int go_c(const LbmDesc& d, const StepParams& P, const void* src, void* dst, int 
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// ------------------------------------------------------------------------- batched lattices
+// One launch advances every lattice of a batch by one step. Work items are warp-sized row
+// segments (32 lanes x V nodes) numbered lattice by lattice; lattice l owns items
+// [item0_l, item0_l + ny_l * segs_l). A warp finds its lattice by binary search over the
+// item offsets (uniform per warp), then runs the single-lattice row code on that lattice's
+// slice of the buffers. Warps stride over the items, so the grid size is a tuning knob.
+template <int STORE, int COLL>
+__global__ void __launch_bounds__(256)
+k_d2q9_batch_ab(const BatchLattice* __restrict__ lats, int nlat, int items,
+                const void* __restrict__ Av, void* __restrict__ Bv) {
+    using E = typename VT<STORE>::E;
+    constexpr int V = VT<STORE>::V;
+    const E* __restrict__ A = static_cast<const E*>(Av);
+    E* __restrict__ B = static_cast<E*>(Bv);
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < items;
+         item += nwarps) {
+        int lo = 0, hi = nlat - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&lats[mid].item0) <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchLattice& bl = lats[lo];
+        const int local = item - __ldg(&bl.item0);
+        const int segs = __ldg(&bl.segs);
+        StepParams P;
+        P.n[0] = __ldg(&bl.nx);
+        P.n[1] = __ldg(&bl.ny);
+        P.n[2] = 1;
+        P.N = P.n[0] * P.n[1];
+        const int per = __ldg(&bl.periodic_mask);
+        P.per[0] = per & 1;
+        P.per[1] = (per >> 1) & 1;
+        P.per[2] = 1;
+        P.ulid = __ldg(&bl.ulid);
+        P.F[0] = P.F[1] = P.F[2] = 0.0f;
+        P.r0 = __ldg(&bl.r0);
+        P.r1 = __ldg(&bl.r1);
+        P.r2 = __ldg(&bl.r2);
+        P.r3 = __ldg(&bl.r3);
+        P.solid = nullptr;
+        P.field = nullptr;
+        P.mx = nullptr;
+        Lane l;
+        l.lane = lane;
+        l.y = local / segs;
+        l.x0 = ((local - l.y * segs) * 32 + lane) * V;
+        l.active = l.x0 < P.n[0];
+        l.first = lane == 0;
+        l.last = l.active && (lane == 31 || l.x0 + V >= P.n[0]);
+        const long long base = __ldg(&bl.base);
+        if (edge_row(P, l.y)) ab_row<STORE, COLL, false, true>(P, A + base, B + base, l);
+        else ab_row<STORE, COLL, false, false>(P, A + base, B + base, l);
+    }
+}
+
+template <int STORE>
+int batch_go(int collision, const BatchLattice* lats, int nlat, int items, const void* src,
+             void* dst, int grid, int block, cudaStream_t s) {
+    switch (collision) {
+        case LBM_BGK:
+            k_d2q9_batch_ab<STORE, LBM_BGK><<<grid, block, 0, s>>>(lats, nlat, items, src, dst);
+            break;
+        case LBM_TRT:
+            k_d2q9_batch_ab<STORE, LBM_TRT><<<grid, block, 0, s>>>(lats, nlat, items, src, dst);
+            break;
+        case LBM_MRT:
+            k_d2q9_batch_ab<STORE, LBM_MRT><<<grid, block, 0, s>>>(lats, nlat, items, src, dst);
+            break;
+        default:
+            return LBM_E_COLLISION;
+    }
+    return int(cudaGetLastError());
+}
+
 }  // namespace
+
+int launch_batch_d2q9(int collision, int storage, const BatchLattice* lats, int nlat,
+                      int items, const void* src, void* dst, int grid, int block,
+                      cudaStream_t s) {
+    switch (storage) {
+        case LBM_STORE_F32:
+            return batch_go<LBM_STORE_F32>(collision, lats, nlat, items, src, dst, grid, block, s);
+        case LBM_STORE_F32_SHIFTED:
+            return batch_go<LBM_STORE_F32_SHIFTED>(collision, lats, nlat, items, src, dst, grid,
+                                                   block, s);
+        case LBM_STORE_F16:
+            return batch_go<LBM_STORE_F16>(collision, lats, nlat, items, src, dst, grid, block, s);
+        case LBM_STORE_BF16:
+            return batch_go<LBM_STORE_BF16>(collision, lats, nlat, items, src, dst, grid, block, s);
+    }
+    return LBM_E_STORAGE;
+}
 
 int launch_fast_d2q9(const LbmDesc& d, const void* src, void* dst, int pattern,
                      cudaStream_t s) {

@@ -73,15 +73,30 @@ def taylor_green_3d_populations(n: int, u0: float = 0.05) -> np.ndarray:
     return equilibrium(D3Q19, rho, u)
 
 
-def cavity_batch(count: int = 64, lo: int = 128, hi: int = 1024, seed: int = 0) -> list[dict]:
-    """Parameters of ``count`` independent lid-driven D2Q9 cavities."""
+def cavity_batch(count: int = 64, lo: int = 128, hi: int = 1024, seed: int = 0,
+                 multiple: int = 8) -> list[dict]:
+    """Parameters of ``count`` independent lid-driven D2Q9 cavities: each edge drawn
+    log-uniform in [lo, hi] and rounded to a multiple of ``multiple`` (rows of whole 16-byte
+    vectors for 16-bit storage), tau ~ U[0.51, 1.0], lid speed ~ U[0.05, 0.1]."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
-        nx, ny = (int(round(np.exp(rng.uniform(np.log(lo), np.log(hi))))) for _ in range(2))
-        out.append({"shape": (nx, ny), "tau": float(rng.uniform(0.51, 1.0)),
+        edges = []
+        for _ in range(2):
+            e = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+            edges.append(int(min(hi, max(lo, multiple * round(e / multiple)))))
+        out.append({"shape": tuple(edges), "tau": float(rng.uniform(0.51, 1.0)),
                     "u_lid": float(rng.uniform(0.05, 0.1))})
     return out
+
+
+def cavity_batch_problems(count: int = 64, lo: int = 128, hi: int = 1024, seed: int = 0,
+                          collision: str = "mrt") -> list:
+    """The batch of :func:`cavity_batch` as Problems (MRT with pylbm's default rates)."""
+    from .problem import Problem
+
+    return [Problem(c["shape"], tau=c["tau"], u_lid=c["u_lid"], collision=collision)
+            for c in cavity_batch(count, lo, hi, seed)]
 
 
 def cylinder_channel(nx: int = 1024, ny: int = 256, xc: float = 200.0, yc: float = 129.0,
