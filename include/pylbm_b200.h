@@ -169,6 +169,21 @@ int lbm_batch_step(LbmBatch* b, void* a, void* bb, int nsteps, uint64_t stream);
  * buffers, step count and launch shape, and cached in the batch */
 int lbm_batch_graph_launch(LbmBatch* b, void* a, void* bb, int nsteps, uint64_t stream);
 
+/* Adjoint of the D2Q9 BGK step (Guo forcing with LbmDesc.force_field, walls, periodic axes,
+ * solids; shifted storages), for the gradient of a momentum-exchange objective with respect
+ * to the per-node force field. No pylbm counterpart (pylbm computes the momentum-exchange
+ * force, karman.py:45-53,88-96, but has no gradients).
+ * lbm_forward_record: one AB step src -> dst that also writes the rho and u its collision
+ *   used, rho_u = 3 planes of N floats (rho, ux, uy): the recomputation pass of checkpointing.
+ * lbm_adjoint_step: one reverse step. lambda_{t+1} = objw * dPhi/df + P^T mu_in (mu_in NULL
+ *   for the last step), mu_out = (dC/dg)^T lambda_{t+1}, grad (2 N doubles) +=
+ *   (dC/dF)^T lambda_{t+1}; rho_u is the record of the forward step t -> t+1; objw is the
+ *   weight of Phi(f_{t+1}) = x momentum-exchange force on the solids in the objective. */
+int lbm_forward_record(const LbmDesc* d, const void* src, void* dst, float* rho_u,
+                       uint64_t stream);
+int lbm_adjoint_step(const LbmDesc* d, const float* rho_u, const float* mu_in, float* mu_out,
+                     double* grad, double objw, uint64_t stream);
+
 /* Tuning of the TMA-staged kernels (D3Q19 always; D2Q9 with LBM_FLAG_STAGED), per lattice and
  * stored element size (2 or 4 bytes), process-wide: nodes per row segment (multiple of 8),
  * shared-memory ring depth (2..8) and consumer warps (1..8). No pylbm counterpart (pylbm

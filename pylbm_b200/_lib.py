@@ -81,6 +81,8 @@ _SIGNATURES = {
     "lbm_batch_get_launch": ([_vp, _vp, _vp], _i),
     "lbm_batch_step": ([_vp, _vp, _vp, _i, _u64], _i),
     "lbm_batch_graph_launch": ([_vp, _vp, _vp, _i, _u64], _i),
+    "lbm_forward_record": ([_d, _vp, _vp, _vp, _u64], _i),
+    "lbm_adjoint_step": ([_d, _vp, _vp, _vp, _vp, ctypes.c_double, _u64], _i),
     "lbm_set_staged_config": ([_i, _i, _i, _i, _i], _i),
     "lbm_get_staged_config": ([_i, _i, _vp, _vp, _vp], _i),
     "lbm_device_error": ([_i], _i),

@@ -32,9 +32,11 @@ namespace lbm {
 // parts with s+ = r0 and s- = r1 directly; BGK relaxes heq_i, heq_o with r0. Same algebra as
 // the per-direction form with about a third fewer instructions: the 16-bit kernels, whose
 // bandwidth needs twice the node rate of fp32, are bound by instruction issue, not HBM.
-template <class L, int COLL, bool FORCE>
+// With MOM, the rho and u the collision uses are also returned (rho_out, u_out[0..D-1]).
+template <class L, int COLL, bool FORCE, bool MOM = false>
 __device__ __forceinline__ void collide_pairs(float (&h)[L::Q], const float (&F)[3], float r0,
-                                              float r1) {
+                                              float r1, float* rho_out = nullptr,
+                                              float* u_out = nullptr) {
     constexpr int Q = L::Q;
     constexpr int D = L::D;
     float a[Q], d[Q];
@@ -69,6 +71,11 @@ __device__ __forceinline__ void collide_pairs(float (&h)[L::Q], const float (&F)
     float u[3];
 #pragma unroll
     for (int ax = 0; ax < D; ++ax) u[ax] = (FORCE ? j[ax] + 0.5f * F[ax] : j[ax]) * inv_rho;
+    if constexpr (MOM) {
+        *rho_out = rho;
+#pragma unroll
+        for (int ax = 0; ax < D; ++ax) u_out[ax] = u[ax];
+    }
     float usq = u[0] * u[0];
 #pragma unroll
     for (int ax = 1; ax < D; ++ax) usq += u[ax] * u[ax];
