@@ -68,7 +68,7 @@ k_forward_record(const StepParams P, const typename Codec<STORE>::T* __restrict_
         F[1] += __ldg(P.field + N + n);
     }
     float rho, u[3];
-    collide_pairs<L, LBM_BGK, FORCE, true>(h, F, P.r0, P.r0, &rho, u);
+    collide<L, LBM_BGK, true, FORCE, C::compact, true>(h, F, P.r0, 0.0f, 0.0f, 0.0f, &rho, u);
     ru[n] = rho;
     ru[N + n] = u[0];
     ru[2 * N + n] = u[1];

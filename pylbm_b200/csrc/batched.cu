@@ -99,7 +99,7 @@ int lbm_batch_create(const LbmDesc* lattices, int count, LbmBatch** out) {
         t.nx = d.nx;
         t.ny = d.ny;
         t.periodic_mask = d.periodic_mask;
-        t.segs = (d.nx / V + 31) / 32;
+        t.segs = d.nx / V;  // vectors per row; a work item is 32 consecutive vectors
         t.item0 = int(items);
         t.ulid = d.ulid;
         t.r0 = d.r0;
@@ -109,7 +109,7 @@ int lbm_batch_create(const LbmDesc* lattices, int count, LbmBatch** out) {
         b->bases.push_back(base);
         base += 9LL * d.nx * d.ny;
         b->nodes += (long long)d.nx * d.ny;
-        items += (long long)d.ny * t.segs;
+        items += ((long long)d.ny * t.segs + 31) / 32;
         if (items >= (1LL << 31)) {
             delete b;
             return LBM_E_SIZE;

@@ -22,6 +22,7 @@ template <>
 struct Codec<LBM_STORE_F32> {
     using T = float;
     static constexpr bool shifted = false;
+    static constexpr bool compact = false;  // 16-bit storage
     __device__ __forceinline__ static float ld(T v) { return v; }
     __device__ __forceinline__ static T st(float v) { return v; }
 };
@@ -30,6 +31,7 @@ template <>
 struct Codec<LBM_STORE_F32_SHIFTED> {
     using T = float;
     static constexpr bool shifted = true;
+    static constexpr bool compact = false;
     __device__ __forceinline__ static float ld(T v) { return v; }
     __device__ __forceinline__ static T st(float v) { return v; }
 };
@@ -38,6 +40,7 @@ template <>
 struct Codec<LBM_STORE_F16> {
     using T = __half;
     static constexpr bool shifted = true;
+    static constexpr bool compact = true;
     __device__ __forceinline__ static float ld(T v) { return __half2float(v); }
     __device__ __forceinline__ static T st(float v) { return __float2half_rn(v); }
 };
@@ -46,6 +49,7 @@ template <>
 struct Codec<LBM_STORE_BF16> {
     using T = __nv_bfloat16;
     static constexpr bool shifted = true;
+    static constexpr bool compact = true;
     __device__ __forceinline__ static float ld(T v) { return __bfloat162float(v); }
     __device__ __forceinline__ static T st(float v) { return __float2bfloat16_rn(v); }
 };

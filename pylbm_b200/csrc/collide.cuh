@@ -24,6 +24,11 @@
 
 namespace lbm {
 
+// Correctly rounded 1/x (the value of the IEEE quotient 1.0f / x) for the shifted
+// collisions. Measured against an approximate reciprocal with one Newton step, it is as fast
+// or faster in every kernel and keeps the reciprocal exact.
+__device__ __forceinline__ float fast_rcp(float x) { return __frcp_rn(x); }
+
 // Shifted BGK / TRT on opposite pairs (i, o = opp(i), c_o = -c_i, w_o = w_i). With the pair
 // sums a = h_i + h_o and differences d = h_i - h_o: drho = h_0 + sum a, j = sum_pairs c_i d,
 // and the equilibrium splits into a symmetric part ep = w (drho + rho (4.5 (c.u)^2 - 1.5 u.u))
@@ -67,7 +72,7 @@ __device__ __forceinline__ void collide_pairs(float (&h)[L::Q], const float (&F)
         }
     }
     const float rho = 1.0f + drho;
-    const float inv_rho = 1.0f / rho;
+    const float inv_rho = fast_rcp(rho);
     float u[3];
 #pragma unroll
     for (int ax = 0; ax < D; ++ax) u[ax] = (FORCE ? j[ax] + 0.5f * F[ax] : j[ax]) * inv_rho;
@@ -165,59 +170,67 @@ __device__ __forceinline__ void collide_mrt_moments(float (&h)[9], const float (
     const float m_pxx = (h[1] + h[3]) - (h[2] + h[4]);
     const float m_pxy = (h[5] + h[7]) - (h[6] + h[8]);
     const float rho = 1.0f + drho;
-    const float inv_rho = 1.0f / rho;
+    const float inv_rho = fast_rcp(rho);
     const float ux = (FORCE ? jx + 0.5f * F[0] : jx) * inv_rho;
     const float uy = (FORCE ? jy + 0.5f * F[1] : jy) * inv_rho;
-    const float usq3 = 3.0f * rho * (ux * ux + uy * uy);
-    float de = -r1 * (m_e - (-2.0f * drho + usq3));
-    float deps = -r2 * (m_eps - (drho - usq3));
-    float dqx = -r3 * (m_qx + rho * ux);
-    float dqy = -r3 * (m_qy + rho * uy);
-    float dpxx = -r0 * (m_pxx - rho * (ux * ux - uy * uy));
-    float dpxy = -r0 * (m_pxy - rho * ux * uy);
-    float djx = 0.0f, djy = 0.0f;
+    const float uxx = ux * ux, uyy = uy * uy;
+    const float usq3 = 3.0f * rho * (uxx + uyy);
+    // relaxed non-equilibrium moments, already divided by the squared row norms
+    // (9, 36, 36, 6, 12, 6, 12, 4, 4): the rates are scaled once, not every moment
+    float ne = (-r1 * (1.0f / 36.0f)) * (m_e - (-2.0f * drho + usq3));
+    float neps = (-r2 * (1.0f / 36.0f)) * (m_eps - (drho - usq3));
+    float nqx = (-r3 * (1.0f / 12.0f)) * (m_qx + rho * ux);
+    float nqy = (-r3 * (1.0f / 12.0f)) * (m_qy + rho * uy);
+    float npxx = (-r0 * 0.25f) * (m_pxx - rho * (uxx - uyy));
+    float npxy = (-r0 * 0.25f) * (m_pxy - rho * ux * uy);
+    float njx = 0.0f, njy = 0.0f;
     if (FORCE) {
         const float uf = ux * F[0] + uy * F[1];
-        de += (1.0f - 0.5f * r1) * (6.0f * uf);
-        deps += (1.0f - 0.5f * r2) * (-6.0f * uf);
-        dqx += (1.0f - 0.5f * r3) * (-F[0]);
-        dqy += (1.0f - 0.5f * r3) * (-F[1]);
-        dpxx += (1.0f - 0.5f * r0) * (2.0f * (ux * F[0] - uy * F[1]));
-        dpxy += (1.0f - 0.5f * r0) * (ux * F[1] + uy * F[0]);
-        djx = F[0];
-        djy = F[1];
+        ne += ((1.0f - 0.5f * r1) * (6.0f / 36.0f)) * uf;
+        neps -= ((1.0f - 0.5f * r2) * (6.0f / 36.0f)) * uf;
+        nqx -= ((1.0f - 0.5f * r3) * (1.0f / 12.0f)) * F[0];
+        nqy -= ((1.0f - 0.5f * r3) * (1.0f / 12.0f)) * F[1];
+        npxx += ((1.0f - 0.5f * r0) * 0.5f) * (ux * F[0] - uy * F[1]);
+        npxy += ((1.0f - 0.5f * r0) * 0.25f) * (ux * F[1] + uy * F[0]);
+        njx = F[0] * (1.0f / 6.0f);
+        njy = F[1] * (1.0f / 6.0f);
     }
-    // back-transform with the squared row norms (9, 36, 36, 6, 12, 6, 12, 4, 4)
-    const float ne = de * (1.0f / 36.0f), neps = deps * (1.0f / 36.0f);
-    const float njx = djx * (1.0f / 6.0f), njy = djy * (1.0f / 6.0f);
-    const float nqx = dqx * (1.0f / 12.0f), nqy = dqy * (1.0f / 12.0f);
-    const float npxx = dpxx * 0.25f, npxy = dpxy * 0.25f;
     const float A = -ne - 2.0f * neps;
     const float Bd = 2.0f * ne + neps;
     const float X = njx - 2.0f * nqx, Y = njy - 2.0f * nqy;
     const float Xd = njx + nqx, Yd = njy + nqy;
-    h[0] += -4.0f * ne + 4.0f * neps;
-    h[1] += A + X + npxx;
-    h[3] += A - X + npxx;
-    h[2] += A + Y - npxx;
-    h[4] += A - Y - npxx;
-    h[5] += Bd + Xd + Yd + npxy;
-    h[6] += Bd - Xd + Yd - npxy;
-    h[7] += Bd - Xd - Yd + npxy;
-    h[8] += Bd + Xd - Yd - npxy;
+    // shared partial sums of the back-transform columns
+    const float ax1 = A + npxx, ax2 = A - npxx;
+    const float dg1 = Bd + npxy, dg2 = Bd - npxy;
+    const float sd = Xd + Yd, dd = Xd - Yd;
+    h[0] += 4.0f * (neps - ne);
+    h[1] += ax1 + X;
+    h[3] += ax1 - X;
+    h[2] += ax2 + Y;
+    h[4] += ax2 - Y;
+    h[5] += dg1 + sd;
+    h[7] += dg1 - sd;
+    h[6] += dg2 - dd;
+    h[8] += dg2 + dd;
 }
 
 // In: f[] pre-collision (h if SHIFT), F = total force at the node (zeros when unforced).
-// Out: f[] post-collision (h* if SHIFT). Shifted storages use the pair / moment-space forms
-// above; the plain form below keeps pylbm's per-direction order (lbm.cu:100-163).
-template <class L, int COLL, bool SHIFT, bool FORCE>
+// Out: f[] post-collision (h* if SHIFT). MRT on shifted storages uses the moment-space form
+// above (measured more accurate against float64 than the per-direction form: 9e-8 vs 1.2e-7
+// on a 500-step cavity). BGK / TRT use the pair form only for COMPACT (16-bit) storages,
+// whose kernels are instruction-bound and whose storage rounding dominates: in fp32 the pair
+// form measured ~3x further from float64 (2.3e-6 vs 0.7e-6 after 1000 cavity steps), so fp32
+// keeps the per-direction form below, which for plain storage is pylbm's order
+// (lbm.cu:100-163). With MOM the rho and u of the collision are also returned.
+template <class L, int COLL, bool SHIFT, bool FORCE, bool COMPACT = false, bool MOM = false>
 __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], float r0,
-                                        float r1, float r2, float r3) {
+                                        float r1, float r2, float r3, float* rho_out = nullptr,
+                                        float* u_out = nullptr) {
     constexpr int Q = L::Q;
     constexpr int D = L::D;
     if constexpr (COLL == LBM_STREAM_ONLY) return;  // debug mode: streaming only
-    if constexpr (SHIFT && (COLL == LBM_BGK || COLL == LBM_TRT)) {
-        collide_pairs<L, COLL, FORCE>(f, F, r0, r1);
+    if constexpr (SHIFT && COMPACT && (COLL == LBM_BGK || COLL == LBM_TRT)) {
+        collide_pairs<L, COLL, FORCE, MOM>(f, F, r0, r1, rho_out, u_out);
         return;
     }
     if constexpr (SHIFT && COLL == LBM_MRT && Q == 9) {
@@ -243,6 +256,11 @@ __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], f
     float u[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int a = 0; a < D; ++a) u[a] = (FORCE ? j[a] + 0.5f * F[a] : j[a]) * inv_rho;
+    if constexpr (MOM) {
+        *rho_out = rho;
+#pragma unroll
+        for (int a = 0; a < D; ++a) u_out[a] = u[a];
+    }
     float usq = u[0] * u[0];
 #pragma unroll
     for (int a = 1; a < D; ++a) usq += u[a] * u[a];

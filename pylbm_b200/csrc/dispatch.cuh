@@ -39,7 +39,7 @@ struct BatchLattice {
     int nx, ny;
     int periodic_mask;
     int item0;          // first warp work item of the lattice
-    int segs;           // warp segments (32 lanes x V nodes) per row
+    int segs;           // V-node vectors per row (a work item is 32 consecutive vectors)
     float ulid, r0, r1, r2, r3;
 };
 

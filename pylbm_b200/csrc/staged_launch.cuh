@@ -93,8 +93,8 @@ __global__ void __launch_bounds__(128) k_aa_even(const StepParams P, void* Av) {
                 f0[i] = p.x;
                 f1[i] = p.y;
             }
-            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f0, F, P.r0, P.r1, P.r2, P.r3);
-            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f1, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, Codec<STORE>::shifted, FORCE, true>(f0, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, Codec<STORE>::shifted, FORCE, true>(f1, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
             for (int i = 0; i < Q; ++i) set_word(v[i], jw, pack2<STORE>(f0[i], f1[i]));
         }

@@ -155,8 +155,8 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[9],
                 f0[i] = LIDS ? p.x + lid[i] : p.x;
                 f1[i] = LIDS ? p.y + lid[i] : p.y;
             }
-            collide<L, COLL, SHIFT, FORCE>(f0, F, P.r0, P.r1, P.r2, P.r3);
-            collide<L, COLL, SHIFT, FORCE>(f1, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, SHIFT, FORCE, true>(f0, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, SHIFT, FORCE, true>(f1, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
             for (int i = 0; i < 9; ++i)
                 set_word(v[i], jw, LIDS ? pack2<STORE>(f0[i] - sub[i], f1[i] - sub[i])
@@ -352,11 +352,15 @@ int go_c(const LbmDesc& d, const StepParams& P, const void* src, void* dst, int 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 // ------------------------------------------------------------------------- batched lattices
-// One launch advances every lattice of a batch by one step. Work items are warp-sized row
-// segments (32 lanes x V nodes) numbered lattice by lattice; lattice l owns items
-// [item0_l, item0_l + ny_l * segs_l). A warp finds its lattice by binary search over the
-// item offsets (uniform per warp), then runs the single-lattice row code on that lattice's
-// slice of the buffers. Warps stride over the items, so the grid size is a tuning knob.
+// One launch advances every lattice of a batch by one step. Each lattice's rows are laid end
+// to end as one sequence of V-node vectors (nx / V per row); a work item is 32 consecutive
+// vectors, one per lane, so rows narrower than a warp do not leave lanes idle. Lattice l owns
+// items [item0_l, item0_l + ceil(nx ny / V / 32)). A warp finds its lattice by binary search
+// over the item offsets (uniform per warp) and runs the single-lattice row code on that
+// lattice's slice of the buffers: the lane at a row start, or at the warp start, takes its
+// x-halo from memory instead of from its neighbour lane. A warp touching a row next to a y
+// wall takes the general (wall and lid) path as a whole. Warps stride over the items, so the
+// grid size is a tuning knob.
 template <int STORE, int COLL>
 __global__ void __launch_bounds__(256)
 k_d2q9_batch_ab(const BatchLattice* __restrict__ lats, int nlat, int items,
@@ -377,7 +381,7 @@ k_d2q9_batch_ab(const BatchLattice* __restrict__ lats, int nlat, int items,
         }
         const BatchLattice& bl = lats[lo];
         const int local = item - __ldg(&bl.item0);
-        const int segs = __ldg(&bl.segs);
+        const int vrow = __ldg(&bl.segs);  // vectors per row
         StepParams P;
         P.n[0] = __ldg(&bl.nx);
         P.n[1] = __ldg(&bl.ny);
@@ -396,15 +400,18 @@ k_d2q9_batch_ab(const BatchLattice* __restrict__ lats, int nlat, int items,
         P.solid = nullptr;
         P.field = nullptr;
         P.mx = nullptr;
+        const int vidx = local * 32 + lane;
+        const int nvec = vrow * P.n[1];
         Lane l;
         l.lane = lane;
-        l.y = local / segs;
-        l.x0 = ((local - l.y * segs) * 32 + lane) * V;
-        l.active = l.x0 < P.n[0];
-        l.first = lane == 0;
-        l.last = l.active && (lane == 31 || l.x0 + V >= P.n[0]);
+        l.active = vidx < nvec;
+        l.y = l.active ? vidx / vrow : 0;
+        l.x0 = l.active ? (vidx - l.y * vrow) * V : 0;
+        l.first = lane == 0 || l.x0 == 0;
+        l.last = l.active && (lane == 31 || l.x0 + V >= P.n[0] || vidx + 1 >= nvec);
         const long long base = __ldg(&bl.base);
-        if (edge_row(P, l.y)) ab_row<STORE, COLL, false, true>(P, A + base, B + base, l);
+        const bool edge = __any_sync(0xffffffffu, l.active && edge_row(P, l.y));
+        if (edge) ab_row<STORE, COLL, false, true>(P, A + base, B + base, l);
         else ab_row<STORE, COLL, false, false>(P, A + base, B + base, l);
     }
 }

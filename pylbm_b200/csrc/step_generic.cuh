@@ -109,7 +109,7 @@ k_step_generic(const StepParams P, const typename Codec<STORE>::T* A,
 #pragma unroll
             for (int a = 0; a < L::D; ++a) F[a] += __ldg(P.field + a * N + n);
         }
-        collide<L, COLL, SHIFT, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+        collide<L, COLL, SHIFT, FORCE, C::compact>(f, F, P.r0, P.r1, P.r2, P.r3);
     }
 
     // ---------------------------------------------------------------- momentum exchange

@@ -151,8 +151,8 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19]
                 f0[i] = LIDS ? p.x + lid[i] : p.x;
                 f1[i] = LIDS ? p.y + lid[i] : p.y;
             }
-            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f0, F, P.r0, P.r1, P.r2, P.r3);
-            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f1, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, Codec<STORE>::shifted, FORCE, true>(f0, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, Codec<STORE>::shifted, FORCE, true>(f1, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
             for (int i = 0; i < 19; ++i) set_word(v[i], jw, pack2<STORE>(f0[i], f1[i]));
         }

@@ -199,7 +199,7 @@ k_staged(const StepParams P, const StagedCfg C, const typename VT<STORE>::E* A,
                 if (wall && top && cx != 0) f[i] += 6.0f * L::w(i) * float(cx) * P.ulid;
             }
             const float F[3] = {P.F[0], P.F[1], P.F[2]};
-            collide<L, COLL, SHIFT, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+            collide<L, COLL, SHIFT, FORCE, Codec<STORE>::compact>(f, F, P.r0, P.r1, P.r2, P.r3);
             if (PATTERN == LBM_PATTERN_AB) {
 #pragma unroll
                 for (int i = 0; i < Q; ++i) __stcs(B + i * N + n, static_cast<E>(T::b(f[i])));
