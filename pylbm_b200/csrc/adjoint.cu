@@ -60,7 +60,7 @@ k_forward_record(const StepParams P, const typename Codec<STORE>::T* __restrict_
             idx = blocked ? L::opp(i) * N + n : i * N + n + off;
         }
         h[i] = C::ld(A[idx]);
-        if (top && L::cx(i) != 0) h[i] += 6.0f * L::w(i) * float(L::cx(i)) * P.ulid;
+        if (top && L::cx(i) != 0) h[i] = add_lid(h[i], lid_term<L>(i, P.ulid));
     }
     float F[3] = {P.F[0], P.F[1], 0.0f};
     if (FORCE && P.field != nullptr) {

@@ -20,198 +20,256 @@
 //    O(|h|) deviations only, which is what keeps 1000 fp32 steps within 1e-6 of float64.
 #pragma once
 
+#include "../../include/pylbm_b200.h"
+#include "f32x2.cuh"
 #include "lattice.cuh"
 
 namespace lbm {
 
-// Correctly rounded 1/x (the value of the IEEE quotient 1.0f / x) for the shifted
-// collisions. Measured against an approximate reciprocal with one Newton step, it is as fast
-// or faster in every kernel and keeps the reciprocal exact.
-__device__ __forceinline__ float fast_rcp(float x) { return __frcp_rn(x); }
+// Ladd's lid term 6 w_i c_ix U of a population pulled from behind the moving top wall, and
+// its addition / removal: explicitly rounded (never fused into an fma), so that every kernel
+// applies it identically, but through intrinsics the compiler can still fold (adding a zero
+// term on the planes without a lid). Its operands are never subnormal.
+template <class L>
+__device__ __forceinline__ float lid_term(int i, float ulid) {
+    return __fmul_rn(6.0f * L::w(i) * float(L::cx(i)), ulid);
+}
+__device__ __forceinline__ float add_lid(float h, float lid) { return __fadd_rn(h, lid); }
+__device__ __forceinline__ float sub_lid(float h, float lid) { return __fsub_rn(h, lid); }
+__device__ __forceinline__ F2 add_lid(F2 h, float lid) {
+    return {__fadd2_rn(h.v, make_float2(lid, lid))};
+}
+__device__ __forceinline__ F2 sub_lid(F2 h, float lid) {
+    return {__fadd2_rn(h.v, make_float2(-lid, -lid))};
+}
+
+// Orientation of an opposite pair (i, opp(i)): the member whose first non-zero velocity
+// component is positive represents the pair, so c.x of a representative never starts with a
+// negation.
+template <class L>
+__device__ __forceinline__ constexpr bool leads_pair(int i) {
+    for (int a = 0; a < L::D; ++a) {
+        const int c = cc<L>(i, a);
+        if (c != 0) return c > 0;
+    }
+    return false;
+}
+
+// Number of non-zero components of c_i, and the first of them.
+template <class L>
+__device__ __forceinline__ constexpr int naxes(int i) {
+    int n = 0;
+    for (int a = 0; a < L::D; ++a) n += cc<L>(i, a) != 0;
+    return n;
+}
+template <class L>
+__device__ __forceinline__ constexpr int first_axis(int i) {
+    for (int a = 0; a < L::D; ++a)
+        if (cc<L>(i, a) != 0) return a;
+    return 0;
+}
+
+// c_i . x for a velocity with unit components: additions and subtractions only.
+template <class L, class S>
+__device__ __forceinline__ S cdot(int i, const S (&x)[3]) {
+    S r = sc<S>(0.0f);
+    bool started = false;
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) {
+        const int c = cc<L>(i, a);
+        if (c == 0) continue;
+        if (!started) r = c > 0 ? x[a] : sc<S>(0.0f) - x[a];
+        else r = c > 0 ? r + x[a] : r - x[a];
+        started = true;
+    }
+    return r;
+}
 
 // Shifted BGK / TRT on opposite pairs (i, o = opp(i), c_o = -c_i, w_o = w_i). With the pair
 // sums a = h_i + h_o and differences d = h_i - h_o: drho = h_0 + sum a, j = sum_pairs c_i d,
 // and the equilibrium splits into a symmetric part ep = w (drho + rho (4.5 (c.u)^2 - 1.5 u.u))
-// and an antisymmetric part em = 3 w rho c.u (heq_i = ep + em, heq_o = ep - em); the Guo
-// source likewise into S+ = w (9 (c.u)(c.F) - 3 u.F) and S- = 3 w c.F. TRT relaxes the two
-// parts with s+ = r0 and s- = r1 directly; BGK relaxes heq_i, heq_o with r0. Same algebra as
-// the per-direction form with about a third fewer instructions: the 16-bit kernels, whose
-// bandwidth needs twice the node rate of fp32, are bound by instruction issue, not HBM.
+// and an antisymmetric part em = 3 w c.(rho u) (heq_i = ep + em, heq_o = ep - em); the Guo
+// source likewise into S+ = w (9 (c.u)(c.F) - 3 u.F) and S- = 3 w c.F (uniform). With s+ = r0
+// and s- = r1 (TRT) or r0 (BGK) the relaxation is written on a and d alone, so h_i, h_o are
+// dead once a, d exist:
+//   p_i = A + B, p_o = A - B,  A = (1 - s+)/2 a + s+ ep + (1 - s+/2) S+,
+//                              B = (1 - s-)/2 d + s- em + (1 - s-/2) S-,
+// which is h_i - s+ (a/2 - ep) - s- (d/2 - em) + ... regrouped. Same algebra as the
+// per-direction form with about a third fewer operations. S is F1 (one node) or F2 (two
+// nodes): the operation sequence, and so every rounding, is the same for both.
+// In this and the MRT form no rounded product feeds an addition or subtraction directly
+// (products enter fma_ or other products only; products by a power of two are exact and
+// exempt): the code generator was measured to fuse such a pair into one fma for the packed
+// instructions but not for the scalar ones, which would make the two types disagree in the
+// last bit. Every F2 constant holds a register pair, so the forms also keep their number
+// small (1 + x and -x are per-node scalar instructions with immediates).
 // With MOM, the rho and u the collision uses are also returned (rho_out, u_out[0..D-1]).
-template <class L, int COLL, bool FORCE, bool MOM = false>
-__device__ __forceinline__ void collide_pairs(float (&h)[L::Q], const float (&F)[3], float r0,
+template <class L, int COLL, bool FORCE, bool MOM = false, class S>
+__device__ __forceinline__ void collide_pairs(S (&h)[L::Q], const float (&F)[3], float r0,
                                               float r1, float* rho_out = nullptr,
                                               float* u_out = nullptr) {
     constexpr int Q = L::Q;
     constexpr int D = L::D;
-    float a[Q], d[Q];
-    float drho = h[0];
+    S a[Q], d[Q];
+    S drho = h[0];
 #pragma unroll
     for (int i = 1; i < Q; ++i) {
+        if (!leads_pair<L>(i)) continue;
         const int o = L::opp(i);
-        if (o < i) continue;
         a[i] = h[i] + h[o];
         d[i] = h[i] - h[o];
-        drho += a[i];
+        drho = drho + a[i];
     }
-    float j[3] = {0.0f, 0.0f, 0.0f};
+    S j[3] = {sc<S>(0.0f), sc<S>(0.0f), sc<S>(0.0f)};
 #pragma unroll
     for (int ax = 0; ax < D; ++ax) {
         bool started = false;
 #pragma unroll
         for (int i = 1; i < Q; ++i) {
-            if (L::opp(i) < i) continue;
+            if (!leads_pair<L>(i)) continue;
             const int c = cc<L>(i, ax);
             if (c == 0) continue;
-            if (!started) {
-                j[ax] = c > 0 ? d[i] : -d[i];
-                started = true;
-            } else {
-                j[ax] = c > 0 ? j[ax] + d[i] : j[ax] - d[i];
-            }
+            if (!started) j[ax] = c > 0 ? d[i] : sc<S>(0.0f) - d[i];
+            else j[ax] = c > 0 ? j[ax] + d[i] : j[ax] - d[i];
+            started = true;
         }
     }
-    const float rho = 1.0f + drho;
-    const float inv_rho = fast_rcp(rho);
-    float u[3];
+    const S rho = one_plus(drho);
+    const S inv_rho = rcp_(rho);
+    S ju[3], u[3];  // ju = rho u = j + F/2
 #pragma unroll
-    for (int ax = 0; ax < D; ++ax) u[ax] = (FORCE ? j[ax] + 0.5f * F[ax] : j[ax]) * inv_rho;
+    for (int ax = 0; ax < 3; ++ax) {
+        ju[ax] = (FORCE && ax < D) ? j[ax] + sc<S>(0.5f * F[ax]) : j[ax];
+        u[ax] = ax < D ? ju[ax] * inv_rho : sc<S>(0.0f);
+    }
     if constexpr (MOM) {
-        *rho_out = rho;
+        *rho_out = scalar_of(rho);
 #pragma unroll
-        for (int ax = 0; ax < D; ++ax) u_out[ax] = u[ax];
+        for (int ax = 0; ax < D; ++ax) u_out[ax] = scalar_of(u[ax]);
     }
-    float usq = u[0] * u[0];
+    S usq = u[0] * u[0];
 #pragma unroll
-    for (int ax = 1; ax < D; ++ax) usq += u[ax] * u[ax];
-    const float t = -1.5f * usq;
-    float uf = 0.0f;
-    if (FORCE) {
-        uf = u[0] * F[0];
+    for (int ax = 1; ax < D; ++ax) usq = fma_(u[ax], u[ax], usq);
+    const S t = sc<S>(-1.5f) * usq;
+    S uf3 = sc<S>(0.0f);  // -3 u.F
+    if constexpr (FORCE) {
+        S uf = u[0] * sc<S>(F[0]);
 #pragma unroll
-        for (int ax = 1; ax < D; ++ax) uf += u[ax] * F[ax];
+        for (int ax = 1; ax < D; ++ax) uf = fma_(u[ax], sc<S>(F[ax]), uf);
+        uf3 = sc<S>(-3.0f) * uf;
     }
+    const float rm = COLL == LBM_TRT ? r1 : r0;
     const float gp = 1.0f - 0.5f * r0;
-    const float gm = 1.0f - 0.5f * (COLL == LBM_TRT ? r1 : r0);
-    {  // rest population
+    const float gm = 1.0f - 0.5f * rm;
+    const float kp = 0.5f * (1.0f - r0);
+    const float km = 0.5f * (1.0f - rm);
+    {  // rest population: heq_0 = w_0 (drho + rho t), S_0 = -3 w_0 u.F
         const float w0 = L::w(0);
-        const float heq = w0 * drho + (w0 * rho) * t;
-        float p = h[0] + r0 * (heq - h[0]);
-        if (FORCE) p += gp * (w0 * (-3.0f * uf));
+        S p = fma_(sc<S>(1.0f - r0), h[0], sc<S>(r0 * w0) * fma_(rho, t, drho));
+        if constexpr (FORCE) p = fma_(sc<S>(gp * w0), uf3, p);
         h[0] = p;
     }
 #pragma unroll
     for (int i = 1; i < Q; ++i) {
+        if (!leads_pair<L>(i)) continue;
         const int o = L::opp(i);
-        if (o < i) continue;
         const float w = L::w(i);
-        float cu = 0.0f, cf = 0.0f;
+        const S cj = cdot<L>(i, ju);  // c.(rho u)
+        // c.u: u_ax itself along an axis, else (c.j) / rho (a product, never a sum of them)
+        const S cu = naxes<L>(i) == 1 ? u[first_axis<L>(i)] : cj * inv_rho;
+        const S x = fma_(rho, fma_(sc<S>(4.5f) * cu, cu, t), drho);  // ep / w
+        S A = fma_(sc<S>(kp), a[i], sc<S>(r0 * w) * x);
+        S B = fma_(sc<S>(km), d[i], sc<S>(rm * 3.0f * w) * cj);
+        if constexpr (FORCE) {
+            float cf = 0.0f;  // c.F (uniform)
 #pragma unroll
-        for (int ax = 0; ax < D; ++ax) {
-            const int c = cc<L>(i, ax);
-            if (c == 1) {
-                cu += u[ax];
-                if (FORCE) cf += F[ax];
-            }
-            if (c == -1) {
-                cu -= u[ax];
-                if (FORCE) cf -= F[ax];
-            }
+            for (int ax = 0; ax < D; ++ax) cf += float(cc<L>(i, ax)) * F[ax];
+            A = fma_(sc<S>(gp), fma_(sc<S>(9.0f * w * cf), cu, sc<S>(w) * uf3), A);
+            B = B + sc<S>(gm * 3.0f * w * cf);
         }
-        const float ep = (w * drho) + (w * rho) * fmaf(4.5f * cu, cu, t);
-        const float em = (3.0f * w * rho) * cu;
-        float sp = 0.0f, sm = 0.0f;
-        if (FORCE) {
-            sp = w * (9.0f * cu * cf - 3.0f * uf);
-            sm = 3.0f * w * cf;
-        }
-        float pi, po;
-        if (COLL == LBM_TRT) {
-            const float np_ = 0.5f * a[i] - ep;
-            const float nm_ = 0.5f * d[i] - em;
-            pi = h[i] - r0 * np_ - r1 * nm_;
-            po = h[o] - r0 * np_ + r1 * nm_;
-            if (FORCE) {
-                pi += gp * sp + gm * sm;
-                po += gp * sp - gm * sm;
-            }
-        } else {
-            pi = h[i] + r0 * ((ep + em) - h[i]);
-            po = h[o] + r0 * ((ep - em) - h[o]);
-            if (FORCE) {
-                pi += gp * (sp + sm);
-                po += gp * (sp - sm);
-            }
-        }
-        h[i] = pi;
-        h[o] = po;
+        h[i] = A + B;
+        h[o] = A - B;
     }
 }
 
 // Shifted D2Q9 MRT in moment space. Moments of h (= M f - M w, M w = (1, -2, 1, 0, ...)) from
 // shared partial sums; equilibrium moments of the second-order feq in closed form,
 // e = -2 drho + 3 rho u.u, eps = drho - 3 rho u.u, q = -rho u, pxx = rho (ux^2 - uy^2),
-// pxy = rho ux uy; Guo source moments M S = (0, 6 u.F, -6 u.F, Fx, -Fx, Fy, -Fy,
-// 2 (ux Fx - uy Fy), ux Fy + uy Fx); then h* = h + M^T (dm / |M_k|^2). Algebraically the
-// update of lattice.py:71-109 / core.py:228-246 with rates (0, r1, r2, 0, r3, 0, r3, r0, r0).
-template <bool FORCE>
-__device__ __forceinline__ void collide_mrt_moments(float (&h)[9], const float (&F)[3],
-                                                    float r0, float r1, float r2, float r3) {
-    const float ax_ = (h[1] + h[3]) + (h[2] + h[4]);
-    const float dg_ = (h[5] + h[7]) + (h[6] + h[8]);
-    const float drho = h[0] + ax_ + dg_;
-    const float m_e = -4.0f * h[0] - ax_ + 2.0f * dg_;
-    const float m_eps = 4.0f * h[0] - 2.0f * ax_ + dg_;
-    const float dx = h[1] - h[3], dy = h[2] - h[4];
-    const float p57 = h[5] - h[7], p86 = h[8] - h[6];
-    const float jx = dx + (p57 + p86), jy = dy + (p57 - p86);
-    const float m_qx = -2.0f * dx + (p57 + p86);
-    const float m_qy = -2.0f * dy + (p57 - p86);
-    const float m_pxx = (h[1] + h[3]) - (h[2] + h[4]);
-    const float m_pxy = (h[5] + h[7]) - (h[6] + h[8]);
-    const float rho = 1.0f + drho;
-    const float inv_rho = fast_rcp(rho);
-    const float ux = (FORCE ? jx + 0.5f * F[0] : jx) * inv_rho;
-    const float uy = (FORCE ? jy + 0.5f * F[1] : jy) * inv_rho;
-    const float uxx = ux * ux, uyy = uy * uy;
-    const float usq3 = 3.0f * rho * (uxx + uyy);
-    // relaxed non-equilibrium moments, already divided by the squared row norms
-    // (9, 36, 36, 6, 12, 6, 12, 4, 4): the rates are scaled once, not every moment
-    float ne = (-r1 * (1.0f / 36.0f)) * (m_e - (-2.0f * drho + usq3));
-    float neps = (-r2 * (1.0f / 36.0f)) * (m_eps - (drho - usq3));
-    float nqx = (-r3 * (1.0f / 12.0f)) * (m_qx + rho * ux);
-    float nqy = (-r3 * (1.0f / 12.0f)) * (m_qy + rho * uy);
-    float npxx = (-r0 * 0.25f) * (m_pxx - rho * (uxx - uyy));
-    float npxy = (-r0 * 0.25f) * (m_pxy - rho * ux * uy);
-    float njx = 0.0f, njy = 0.0f;
-    if (FORCE) {
-        const float uf = ux * F[0] + uy * F[1];
-        ne += ((1.0f - 0.5f * r1) * (6.0f / 36.0f)) * uf;
-        neps -= ((1.0f - 0.5f * r2) * (6.0f / 36.0f)) * uf;
-        nqx -= ((1.0f - 0.5f * r3) * (1.0f / 12.0f)) * F[0];
-        nqy -= ((1.0f - 0.5f * r3) * (1.0f / 12.0f)) * F[1];
-        npxx += ((1.0f - 0.5f * r0) * 0.5f) * (ux * F[0] - uy * F[1]);
-        npxy += ((1.0f - 0.5f * r0) * 0.25f) * (ux * F[1] + uy * F[0]);
-        njx = F[0] * (1.0f / 6.0f);
-        njy = F[1] * (1.0f / 6.0f);
+// pxy = rho ux uy, with rho u = j + F/2 used directly; Guo source moments
+// M S = (0, 6 u.F, -6 u.F, Fx, -Fx, Fy, -Fy, 2 (ux Fx - uy Fy), ux Fy + uy Fx); then
+// h* = h + M^T (dm / |M_k|^2). Algebraically the update of lattice.py:71-109 /
+// core.py:228-246 with rates (0, r1, r2, 0, r3, 0, r3, r0, r0). S is float (fp32 storages),
+// F1 or F2 (16-bit storages, identical roundings; see collide_pairs for the rules kept).
+template <bool FORCE, class S>
+__device__ __forceinline__ void collide_mrt_moments(S (&h)[9], const float (&F)[3], float r0,
+                                                    float r1, float r2, float r3) {
+    const S s13 = h[1] + h[3], s24 = h[2] + h[4];
+    const S s57 = h[5] + h[7], s68 = h[6] + h[8];
+    const S ax_ = s13 + s24, dg_ = s57 + s68;
+    const S drho = (h[0] + ax_) + dg_;
+    // (-4 h0 is exact, so whether it is fused with the subtraction does not change the value)
+    const S m_e = fma_(sc<S>(2.0f), dg_, sc<S>(-4.0f) * h[0] - ax_);
+    const S m_eps = fma_(sc<S>(4.0f), h[0], fma_(sc<S>(-2.0f), ax_, dg_));
+    const S dx = h[1] - h[3], dy = h[2] - h[4];
+    const S p57 = h[5] - h[7], p86 = h[8] - h[6];
+    const S q1 = p57 + p86, q2 = p57 - p86;
+    const S m_qx = fma_(sc<S>(-2.0f), dx, q1);
+    const S m_qy = fma_(sc<S>(-2.0f), dy, q2);
+    const S m_pxx = s13 - s24;
+    const S m_pxy = s57 - s68;
+    const S inv_rho = rcp_(one_plus(drho));
+    const S jux = FORCE ? (dx + q1) + sc<S>(0.5f * F[0]) : dx + q1;  // rho u
+    const S juy = FORCE ? (dy + q2) + sc<S>(0.5f * F[1]) : dy + q2;
+    const S ux = jux * inv_rho, uy = juy * inv_rho;
+    const S nux = jux * neg_(inv_rho);  // -ux
+    const S usq3 = sc<S>(3.0f) * fma_(jux, ux, juy * uy);  // 3 rho u.u
+    // relaxed non-equilibrium moments divided by the squared row norms
+    // (9, 36, 36, 6, 12, 6, 12, 4, 4); nne = -dm_e
+    const float ceps = -r2 * (1.0f / 36.0f), cq = -r3 * (1.0f / 12.0f), cp = -r0 * 0.25f;
+    S nne = sc<S>(r1 * (1.0f / 36.0f)) * (m_e - fma_(sc<S>(-2.0f), drho, usq3));
+    S neps = fma_(sc<S>(ceps), m_eps - drho, sc<S>(ceps) * usq3);
+    S nqx = fma_(sc<S>(cq), m_qx, sc<S>(cq) * jux);
+    S nqy = fma_(sc<S>(cq), m_qy, sc<S>(cq) * juy);
+    // pxx_eq = rho (ux^2 - uy^2) = jux ux - juy uy, pxy_eq = rho ux uy = ux juy
+    S npxx = fma_(sc<S>(cp), fma_(juy, uy, m_pxx), sc<S>(cp) * (jux * nux));
+    S npxy = fma_(sc<S>(cp), m_pxy, sc<S>(cp) * (nux * juy));
+    S X, Y, Xd, Yd;
+    if constexpr (FORCE) {
+        const S uf = fma_(ux, sc<S>(F[0]), uy * sc<S>(F[1]));
+        nne = fma_(sc<S>(-(1.0f - 0.5f * r1) * (6.0f / 36.0f)), uf, nne);
+        neps = fma_(sc<S>(-(1.0f - 0.5f * r2) * (6.0f / 36.0f)), uf, neps);
+        nqx = nqx - sc<S>((1.0f - 0.5f * r3) * (1.0f / 12.0f) * F[0]);
+        nqy = nqy - sc<S>((1.0f - 0.5f * r3) * (1.0f / 12.0f) * F[1]);
+        npxx = fma_(sc<S>((1.0f - 0.5f * r0) * 0.5f),
+                    fma_(ux, sc<S>(F[0]), sc<S>(-F[1]) * uy), npxx);
+        npxy = fma_(sc<S>((1.0f - 0.5f * r0) * 0.25f),
+                    fma_(ux, sc<S>(F[1]), uy * sc<S>(F[0])), npxy);
+        const float njx = F[0] * (1.0f / 6.0f), njy = F[1] * (1.0f / 6.0f);
+        X = fma_(sc<S>(-2.0f), nqx, sc<S>(njx));
+        Y = fma_(sc<S>(-2.0f), nqy, sc<S>(njy));
+        Xd = nqx + sc<S>(njx);
+        Yd = nqy + sc<S>(njy);
+    } else {
+        X = sc<S>(-2.0f) * nqx;  // exact
+        Y = sc<S>(-2.0f) * nqy;
+        Xd = nqx;
+        Yd = nqy;
     }
-    const float A = -ne - 2.0f * neps;
-    const float Bd = 2.0f * ne + neps;
-    const float X = njx - 2.0f * nqx, Y = njy - 2.0f * nqy;
-    const float Xd = njx + nqx, Yd = njy + nqy;
+    const S A = fma_(sc<S>(-2.0f), neps, nne);   // -dm_e - 2 dm_eps
+    const S Bd = fma_(sc<S>(-2.0f), nne, neps);  // 2 dm_e + dm_eps
     // shared partial sums of the back-transform columns
-    const float ax1 = A + npxx, ax2 = A - npxx;
-    const float dg1 = Bd + npxy, dg2 = Bd - npxy;
-    const float sd = Xd + Yd, dd = Xd - Yd;
-    h[0] += 4.0f * (neps - ne);
-    h[1] += ax1 + X;
-    h[3] += ax1 - X;
-    h[2] += ax2 + Y;
-    h[4] += ax2 - Y;
-    h[5] += dg1 + sd;
-    h[7] += dg1 - sd;
-    h[6] += dg2 - dd;
-    h[8] += dg2 + dd;
+    const S ax1 = A + npxx, ax2 = A - npxx;
+    const S dg1 = Bd + npxy, dg2 = Bd - npxy;
+    const S sd = Xd + Yd, dd = Xd - Yd;
+    h[0] = fma_(sc<S>(4.0f), neps, fma_(sc<S>(4.0f), nne, h[0]));
+    h[1] = h[1] + (ax1 + X);
+    h[3] = h[3] + (ax1 - X);
+    h[2] = h[2] + (ax2 + Y);
+    h[4] = h[4] + (ax2 - Y);
+    h[5] = h[5] + (dg1 + sd);
+    h[7] = h[7] + (dg1 - sd);
+    h[6] = h[6] + (dg2 - dd);
+    h[8] = h[8] + (dg2 + dd);
 }
 
 // In: f[] pre-collision (h if SHIFT), F = total force at the node (zeros when unforced).
@@ -221,7 +279,8 @@ __device__ __forceinline__ void collide_mrt_moments(float (&h)[9], const float (
 // whose kernels are instruction-bound and whose storage rounding dominates: in fp32 the pair
 // form measured ~3x further from float64 (2.3e-6 vs 0.7e-6 after 1000 cavity steps), so fp32
 // keeps the per-direction form below, which for plain storage is pylbm's order
-// (lbm.cu:100-163). With MOM the rho and u of the collision are also returned.
+// (lbm.cu:100-163). COMPACT collisions run in F1 arithmetic, bit-for-bit what collide2 gives
+// the packed 16-bit kernels. With MOM the rho and u of the collision are also returned.
 template <class L, int COLL, bool SHIFT, bool FORCE, bool COMPACT = false, bool MOM = false>
 __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], float r0,
                                         float r1, float r2, float r3, float* rho_out = nullptr,
@@ -229,8 +288,19 @@ __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], f
     constexpr int Q = L::Q;
     constexpr int D = L::D;
     if constexpr (COLL == LBM_STREAM_ONLY) return;  // debug mode: streaming only
-    if constexpr (SHIFT && COMPACT && (COLL == LBM_BGK || COLL == LBM_TRT)) {
-        collide_pairs<L, COLL, FORCE, MOM>(f, F, r0, r1, rho_out, u_out);
+    if constexpr (SHIFT && COMPACT &&
+                  (COLL == LBM_BGK || COLL == LBM_TRT || (COLL == LBM_MRT && Q == 9))) {
+        F1 g[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i].v = f[i];
+        if constexpr (COLL == LBM_MRT) {
+            static_assert(!MOM, "rho / u output is implemented for BGK and TRT");
+            collide_mrt_moments<FORCE>(g, F, r0, r1, r2, r3);
+        } else {
+            collide_pairs<L, COLL, FORCE, MOM>(g, F, r0, r1, rho_out, u_out);
+        }
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = g[i].v;
         return;
     }
     if constexpr (SHIFT && COLL == LBM_MRT && Q == 9) {
@@ -358,6 +428,25 @@ __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], f
             }
             f[i] = acc;
         }
+    }
+}
+
+}  // namespace lbm
+
+namespace lbm {
+
+// Two nodes of a 16-bit storage word at once (packed fp32 pairs, shifted arithmetic):
+// bit-for-bit collide<L, COLL, true, FORCE, true> applied to each node.
+template <class L, int COLL, bool FORCE>
+__device__ __forceinline__ void collide2(F2 (&f)[L::Q], const float (&F)[3], float r0,
+                                         float r1, float r2, float r3) {
+    if constexpr (COLL == LBM_STREAM_ONLY) {
+        return;
+    } else if constexpr (COLL == LBM_MRT) {
+        static_assert(L::Q == 9, "MRT is implemented for D2Q9 only");
+        collide_mrt_moments<FORCE>(f, F, r0, r1, r2, r3);
+    } else {
+        collide_pairs<L, COLL, FORCE>(f, F, r0, r1);
     }
 }
 

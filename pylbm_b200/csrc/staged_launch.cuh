@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(128) k_aa_even(const StepParams P, void* Av) {
 #pragma unroll
             for (int i = 0; i < Q; ++i) put<V>(v[i], k, T::b(f[i]));
         }
-    } else {  // 16-bit: two nodes per word, packed conversions
+    } else {  // 16-bit: two nodes per word, collided one after the other (see step_rows3d.cuh)
 #pragma unroll
         for (int jw = 0; jw < 4; ++jw) {
             float f0[Q], f1[Q];

@@ -38,11 +38,6 @@ using L = D2Q9;
 constexpr int kThreads = 128;
 constexpr unsigned kFull = 0xffffffffu;
 
-// Lid term 6 w_i c_ix U for a pull whose source is behind the top wall.
-__device__ __forceinline__ float lid_term(int i, float ulid) {
-    return 6.0f * L::w(i) * float(L::cx(i)) * ulid;
-}
-
 // Row y - cy, wrapped. EDGE rows also report whether the row lies behind a wall (then it is
 // not wrapped) and whether that wall is the top one.
 template <bool EDGE>
@@ -81,7 +76,7 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
         const int bb_slot = READ_OPP ? i : L::opp(i);
         bool wall, top;
         const int ys = src_row<EDGE>(y, cy, ny, pery, wall, top);
-        lid[i] = (wall && top && cx != 0) ? lid_term(i, P.ulid) : 0.0f;
+        lid[i] = (wall && top && cx != 0) ? lid_term<L>(i, P.ulid) : 0.0f;
         v[i] = make_uint4(0u, 0u, 0u, 0u);
         halo[i] = 0u;
         if (!active) continue;
@@ -139,28 +134,28 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[9],
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
                 f[i] = T::f(elem<V>(v[i], k));
-                if (LIDS) f[i] += lid[i];
+                if (LIDS) f[i] = add_lid(f[i], lid[i]);
             }
             collide<L, COLL, SHIFT, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) put<V>(v[i], k, T::b(LIDS ? f[i] - sub[i] : f[i]));
+            for (int i = 0; i < 9; ++i)
+                put<V>(v[i], k, T::b(LIDS ? sub_lid(f[i], sub[i]) : f[i]));
         }
-    } else {  // 16-bit: two nodes per word, packed conversions
+    } else {  // 16-bit: the two nodes of a word at once, packed conversions and arithmetic
 #pragma unroll
         for (int jw = 0; jw < 4; ++jw) {
-            float f0[9], f1[9];
+            F2 f[9];
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
-                const float2 p = unpack2<STORE>(word(v[i], jw));
-                f0[i] = LIDS ? p.x + lid[i] : p.x;
-                f1[i] = LIDS ? p.y + lid[i] : p.y;
+                f[i].v = unpack2<STORE>(word(v[i], jw));
+                if (LIDS) f[i] = add_lid(f[i], lid[i]);
             }
-            collide<L, COLL, SHIFT, FORCE, true>(f0, F, P.r0, P.r1, P.r2, P.r3);
-            collide<L, COLL, SHIFT, FORCE, true>(f1, F, P.r0, P.r1, P.r2, P.r3);
+            collide2<L, COLL, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
-            for (int i = 0; i < 9; ++i)
-                set_word(v[i], jw, LIDS ? pack2<STORE>(f0[i] - sub[i], f1[i] - sub[i])
-                                        : pack2<STORE>(f0[i], f1[i]));
+            for (int i = 0; i < 9; ++i) {
+                if (LIDS) f[i] = sub_lid(f[i], sub[i]);
+                set_word(v[i], jw, pack2<STORE>(f[i].v.x, f[i].v.y));
+            }
         }
     }
 }
@@ -248,7 +243,7 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
         bool wall, top;
         drow[i] = src_row<EDGE>(l.y, -L::cy(i), ny, P.per[1], wall, top);
         dwall[i] = wall;
-        sub[i] = (wall && top && L::cx(i) != 0) ? lid_term(i, P.ulid) : 0.0f;
+        sub[i] = (wall && top && L::cx(i) != 0) ? lid_term<L>(i, P.ulid) : 0.0f;
     }
     if (l.active) collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid, sub);
     const int own = l.y * nx + l.x0;

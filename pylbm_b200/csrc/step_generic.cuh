@@ -101,7 +101,7 @@ k_step_generic(const StepParams P, const typename Codec<STORE>::T* A,
                     idx = blocked ? i * N + n : L::opp(i) * N + n + off;
             }
             f[i] = C::ld(A[idx]);
-            if (top && L::cx(i) != 0) f[i] += 6.0f * L::w(i) * float(L::cx(i)) * P.ulid;
+            if (top && L::cx(i) != 0) f[i] = add_lid(f[i], lid_term<L>(i, P.ulid));
         }
         // ------------------------------------------------------------ collide
         float F[3] = {P.F[0], P.F[1], P.F[2]};
@@ -152,7 +152,7 @@ k_step_generic(const StepParams P, const typename Codec<STORE>::T* A,
             const int off = link<L>(P, crd, i, +1, wall, top);
             if (wall) {
                 float v = f[i];
-                if (top && L::cx(i) != 0) v -= 6.0f * L::w(i) * float(L::cx(i)) * P.ulid;
+                if (top && L::cx(i) != 0) v = sub_lid(v, lid_term<L>(i, P.ulid));
                 B[L::opp(i) * N + n] = C::st(v);
             } else {
                 B[i * N + n + off] = C::st(f[i]);

@@ -82,7 +82,7 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
         const int bb_slot = READ_OPP ? i : L::opp(i);
         bool wall, top;
         const int r = src_row<EDGE>(P, l.y, l.z, L::cy(i), L::cz(i), wall, top);
-        lid[i] = (wall && top && cx != 0) ? 6.0f * L::w(i) * float(cx) * P.ulid : 0.0f;
+        lid[i] = (wall && top && cx != 0) ? lid_term<L>(i, P.ulid) : 0.0f;
         v[i] = make_uint4(0u, 0u, 0u, 0u);
         halo[i] = 0u;
         if (!l.active) continue;
@@ -135,21 +135,26 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19]
 #pragma unroll
             for (int i = 0; i < 19; ++i) {
                 f[i] = T::f(elem<V>(v[i], k));
-                if (LIDS) f[i] += lid[i];
+                if (LIDS) f[i] = add_lid(f[i], lid[i]);
             }
             collide<L, COLL, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
             for (int i = 0; i < 19; ++i) put<V>(v[i], k, T::b(f[i]));
         }
-    } else {  // 16-bit: two nodes per word, packed conversions
+    } else {
+        // 16-bit: two nodes per word, packed conversions, the two nodes collided one after the
+        // other (F1 arithmetic, bit-for-bit the packed F2 result). The packed form needs ~45
+        // more registers here (19 populations of two nodes live at once on top of the 76
+        // registers of loaded rows), which drops this latency-bound kernel from 3 to 2
+        // resident blocks per SM: measured 15% slower.
 #pragma unroll
         for (int jw = 0; jw < 4; ++jw) {
             float f0[19], f1[19];
 #pragma unroll
             for (int i = 0; i < 19; ++i) {
                 const float2 p = unpack2<STORE>(word(v[i], jw));
-                f0[i] = LIDS ? p.x + lid[i] : p.x;
-                f1[i] = LIDS ? p.y + lid[i] : p.y;
+                f0[i] = LIDS ? add_lid(p.x, lid[i]) : p.x;
+                f1[i] = LIDS ? add_lid(p.y, lid[i]) : p.y;
             }
             collide<L, COLL, Codec<STORE>::shifted, FORCE, true>(f0, F, P.r0, P.r1, P.r2, P.r3);
             collide<L, COLL, Codec<STORE>::shifted, FORCE, true>(f1, F, P.r0, P.r1, P.r2, P.r3);

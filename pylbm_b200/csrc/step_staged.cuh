@@ -196,7 +196,7 @@ k_staged(const StepParams P, const StagedCfg C, const typename VT<STORE>::E* A,
                     raw = uint32_t(st[i * pitch + H + xl - (wall ? 0 : cx)]);
                 }
                 f[i] = T::f(raw);
-                if (wall && top && cx != 0) f[i] += 6.0f * L::w(i) * float(cx) * P.ulid;
+                if (wall && top && cx != 0) f[i] = add_lid(f[i], lid_term<L>(i, P.ulid));
             }
             const float F[3] = {P.F[0], P.F[1], P.F[2]};
             collide<L, COLL, SHIFT, FORCE, Codec<STORE>::compact>(f, F, P.r0, P.r1, P.r2, P.r3);
@@ -224,7 +224,7 @@ k_staged(const StepParams P, const StagedCfg C, const typename VT<STORE>::E* A,
                     }
                     if (wall) {
                         float v = f[i];
-                        if (top && L::cx(i) != 0) v -= 6.0f * L::w(i) * float(L::cx(i)) * P.ulid;
+                        if (top && L::cx(i) != 0) v = sub_lid(v, lid_term<L>(i, P.ulid));
                         B[L::opp(i) * N + n] = static_cast<E>(T::b(v));
                     } else {
                         B[i * N + n + off] = static_cast<E>(T::b(f[i]));
