@@ -7,6 +7,11 @@ shifted arithmetic), pull two-buffer; rho = 1 + 0.01 N(0,1), u = 8 seeded Fourie
 max|u| = 0.05. One benchmark step = 1000 lattice time steps of the whole lattice. The state
 (2 x 604 MB) is larger than L2, so no flush is needed between steps.
 
+Batched workload ``d2q9-mrt-batch64-f16``: 64 independent D2Q9 MRT lid-driven cavities, edges
+log-uniform in [128, 1024] (multiples of 8), tau ~ U[0.51, 1], lid speed ~ U[0.05, 0.1], fp16
+storage, advanced together by one launch per lattice step; one benchmark step = 2000 lattice
+steps replayed from one CUDA graph (2 x 209 MB of state, larger than L2).
+
 * ``value``    MLUPS with the state resident in HBM, CUDA events on the launching stream,
                max over ranks (replicas: every rank advances its own lattice, no collective
                on the data path).
@@ -60,8 +65,36 @@ WORKLOADS = {
 }
 
 
+# batches of independent lattices: name -> (count, collision, variant, seed)
+BATCHES = {
+    "d2q9-mrt-batch64-f16": (64, "mrt", "fused-fp16", 0),
+}
+
+
 def is_cavity(name: str) -> bool:
     return "cavity" in name
+
+
+def batch_problems(name: str) -> list:
+    from pylbm_b200 import workloads as W
+
+    count, coll, _, seed = BATCHES[name]
+    return W.cavity_batch_problems(count, seed=seed, collision=coll)
+
+
+def dominant_kernel(name: str) -> str:
+    """The step kernel the workload runs (the only kernel launched in the timed region)."""
+    if name in BATCHES:
+        return "k_d2q9_batch_ab"
+    lat, _, _, _, variant = WORKLOADS[name]
+    if "-aa" in variant:
+        return ("k_d2q9_aa_odd + k_d2q9_aa_even" if lat == "D2Q9"
+                else "k_staged (AA odd) + k_aa_even")
+    return "k_d2q9_ab" if lat == "D2Q9" else "rows3d::k_ab"
+
+
+def default_lbm_steps(name: str) -> int:
+    return 2000 if name in BATCHES else 1000
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -193,6 +226,26 @@ def _oracle_band_worker(args: tuple) -> float:
     return time.perf_counter() - t0
 
 
+def _oracle_batch_worker(args: tuple) -> tuple[float, int]:
+    """Time ``steps`` oracle steps on lattice ``i`` of a batch (runs in a spawned process);
+    returns (seconds, nodes)."""
+    name, i, steps, warmup, barrier = args
+    sys.path.insert(0, str(ROOT))
+    from oracle import lbm_oracle as O
+
+    p = batch_problems(name)[i]
+    case = O.Case(tuple(p.shape), p.tau, p.collision, (False, False), u_lid=p.u_lid)
+    f = p.initial_populations()
+    for _ in range(warmup):
+        f = O.step(f, case)
+    if barrier is not None:
+        barrier.wait()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        f = O.step(f, case)
+    return time.perf_counter() - t0, p.n_nodes
+
+
 def band_nodes(name: str, rows: int) -> int:
     lat, n, *_ = WORKLOADS[name]
     return n * rows if lat == "D2Q9" else n * n * rows
@@ -200,6 +253,11 @@ def band_nodes(name: str, rows: int) -> int:
 
 def cpu_baseline(name: str) -> dict:
     """The oracle on one core, a bounded sample of the workload (about 10 s)."""
+    if name in BATCHES:
+        dt, nodes = _oracle_batch_worker((name, 0, 3, 1, None))
+        return {"value": nodes * 3 / dt / 1e6, "unit": "MLUPS", "cores": 1, "kind": "port",
+                "sample": f"float64 NumPy oracle, 3 steps of lattice 0 of the batch "
+                          f"({nodes} nodes)"}
     lat = WORKLOADS[name][0]
     rows, steps = (512, 3) if lat == "D2Q9" else (8, 3)
     dt = _oracle_band_worker((name, rows, steps, 1, 0, None))
@@ -217,20 +275,30 @@ def run_reference(a: argparse.Namespace) -> None:
     if rank != 0:
         return
     name = a.workload
-    lat = WORKLOADS[name][0]
     cores = min(os.cpu_count() or 1, a.cpu_procs)
-    rows = 64 if lat == "D2Q9" else 2
     ctx = mp.get_context("spawn")
     mgr = ctx.Manager()
     barrier = mgr.Barrier(cores)
-    with ctx.Pool(cores) as pool:
-        times = pool.map(_oracle_band_worker,
-                         [(name, rows, a.steps, a.warmup, 0, barrier)] * cores)
-    dt = max(times)
-    total = cores * band_nodes(name, rows) * a.steps
+    if name in BATCHES:  # one lattice of the batch per process
+        count = BATCHES[name][0]
+        with ctx.Pool(cores) as pool:
+            res = pool.map(_oracle_batch_worker,
+                           [(name, i % count, a.steps, a.warmup, barrier) for i in range(cores)])
+        dt = max(r[0] for r in res)
+        total = sum(r[1] for r in res) * a.steps
+        sample = (f"float64 NumPy oracle, {cores} processes x {a.steps} steps, each on one "
+                  f"lattice of the batch")
+    else:
+        lat = WORKLOADS[name][0]
+        rows = 64 if lat == "D2Q9" else 2
+        with ctx.Pool(cores) as pool:
+            times = pool.map(_oracle_band_worker,
+                             [(name, rows, a.steps, a.warmup, 0, barrier)] * cores)
+        dt = max(times)
+        total = cores * band_nodes(name, rows) * a.steps
+        sample = (f"float64 NumPy oracle, {cores} processes x {a.steps} steps of a periodic "
+                  f"band of {band_nodes(name, rows)} nodes each")
     mlups = total / dt / 1e6
-    sample = (f"float64 NumPy oracle, {cores} processes x {a.steps} steps of a periodic band "
-              f"of {band_nodes(name, rows)} nodes each")
     out = {"impl": "reference", "metric": "MLUPS", "value": mlups, "unit": "MLUPS",
            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": 1e3 * dt / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -244,6 +312,17 @@ def run_reference(a: argparse.Namespace) -> None:
 
 
 def config_of(name: str, a: argparse.Namespace) -> dict:
+    if name in BATCHES:
+        count, coll, variant, seed = BATCHES[name]
+        probs = batch_problems(name)
+        return {"workload": name, "lattice": "D2Q9", "lattices": count,
+                "nodes": int(sum(p.n_nodes for p in probs)), "collision": coll,
+                "variant": variant, "edges": "log-uniform [128, 1024], multiples of 8",
+                "tau": "U[0.51, 1.0]", "u_lid": "U[0.05, 0.1]", "seed": seed,
+                "lbm_steps_per_step": a.lbm_steps, "launch": "CUDA graph, one launch per step",
+                "init": "lid-driven cavities, fluid at rest",
+                "l2": "state larger than L2 (no flush needed)",
+                "parallelism": f"replicas x{a.gpus}"}
     lat, n, coll, tau, variant = WORKLOADS[name]
     n = a.n or n
     shape = [n, n] if lat == "D2Q9" else [n, n, n]
@@ -275,12 +354,20 @@ def run_b200(a: argparse.Namespace) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     name = a.workload
-    cls = VARIANTS[WORKLOADS[name][4]]
-    p = make_problem(name, a.n)
-    s = cls(p)
-    s.set_populations(initial_state(name, seed=rank, n=a.n))
+    if name in BATCHES:
+        from pylbm_b200.autotune import autotune_batch
+        from pylbm_b200.batched import BatchedSolver
+
+        s = BatchedSolver(batch_problems(name), BATCHES[name][2])
+        autotune_batch(s)
+        nodes = s.nodes
+    else:
+        cls = VARIANTS[WORKLOADS[name][4]]
+        p = make_problem(name, a.n)
+        s = cls(p)
+        s.set_populations(initial_state(name, seed=rank, n=a.n))
+        nodes = p.n_nodes
     L = a.lbm_steps
-    nodes = p.n_nodes
 
     def barrier() -> None:
         torch.cuda.synchronize()
@@ -350,7 +437,8 @@ def run_b200(a: argparse.Namespace) -> None:
             "dtype": "f32" if s.storage == "f32" else s.storage, "data": "synthetic",
             "config": config_of(name, a),
             "bytes_per_update": bpn, "effective_GBs": value * 1e6 * bpn / 1e9,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": dominant_kernel(name),
+                         "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": bpn * nodes},
             "gpu_launches": launches,
@@ -372,14 +460,19 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="d2q9-bgk-ab-f32", choices=sorted(WORKLOADS))
-    ap.add_argument("--lbm-steps", type=int, default=1000,
-                    help="lattice time steps per benchmark step")
+    ap.add_argument("--workload", default="d2q9-bgk-ab-f32",
+                    choices=sorted(WORKLOADS) + sorted(BATCHES))
+    ap.add_argument("--lbm-steps", type=int, default=None,
+                    help="lattice time steps per benchmark step (1000; 2000 for batches)")
     ap.add_argument("--n", type=int, default=None, help="override the lattice edge (profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=64)
     a = ap.parse_args()
+    if a.lbm_steps is None:
+        a.lbm_steps = default_lbm_steps(a.workload)
+    if a.workload in BATCHES and a.n is not None:
+        ap.error("--n does not apply to batches")
     if a.warmup < 3 and a.impl == "b200":
         log("note: fewer than 3 warm-up steps")
     if a.impl == "reference":

@@ -160,7 +160,9 @@ int lbm_batch_create(const LbmDesc* lattices, int count, LbmBatch** out);
 int lbm_batch_destroy(LbmBatch* b);
 int lbm_batch_info(const LbmBatch* b, int64_t* elements, int64_t* nodes, int* items);
 int lbm_batch_offsets(const LbmBatch* b, int64_t* offsets);
-/* launch shape, chosen by the autotuner: threads per block (64/128/256), blocks per SM */
+/* launch shape, chosen by the autotuner: threads per block (64/128/256) and resident blocks
+ * per SM (1..64: a persistent grid whose warps stride over the work items; 0: one work item
+ * per warp) */
 int lbm_batch_set_launch(LbmBatch* b, int block, int blocks_per_sm);
 int lbm_batch_get_launch(const LbmBatch* b, int* block, int* blocks_per_sm);
 /* nsteps pull steps, ping-pong a -> b -> a ...: the result is in a when nsteps is even */

@@ -18,7 +18,7 @@ from pathlib import Path
 from typing import Any, Callable, Iterable
 
 BLOCKS = (64, 128, 256)
-PER_SM = (2, 4, 8, 16, 32)
+PER_SM = (0, 2, 4, 8, 16, 32)  # resident blocks per SM; 0 = one work item per warp
 
 
 def cache_path() -> Path:

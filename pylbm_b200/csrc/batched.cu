@@ -24,6 +24,7 @@ struct LbmBatch {
     long long nodes = 0;
     std::vector<long long> bases;
     lbm::BatchLattice* table = nullptr;  // device
+    uint16_t* item_lat = nullptr;         // device, lattice of every work item
     int block = 256;
     int blocks_per_sm = 8;
     int sms = 0;
@@ -40,9 +41,10 @@ int vec_elems(int storage) {
     return (storage == LBM_STORE_F16 || storage == LBM_STORE_BF16) ? 8 : 4;
 }
 
+// blocks_per_sm = 0: one work item per warp (no grid-stride loop)
 int grid_of(const LbmBatch& b) {
-    long long g = (long long)b.blocks_per_sm * b.sms;
     const long long need = ((long long)b.items * 32 + b.block - 1) / b.block;
+    long long g = b.blocks_per_sm > 0 ? (long long)b.blocks_per_sm * b.sms : need;
     if (g > need) g = need;
     return int(g < 1 ? 1 : g);
 }
@@ -52,8 +54,9 @@ int launch_steps(LbmBatch* b, void* a, void* bb, int nsteps, cudaStream_t s) {
     for (int k = 0; k < nsteps; ++k) {
         const void* src = (k & 1) ? bb : a;
         void* dst = (k & 1) ? a : bb;
-        const int rc = lbm::launch_batch_d2q9(b->collision, b->storage, b->table, b->count,
-                                              b->items, src, dst, grid, b->block, s);
+        const int rc = lbm::launch_batch_d2q9(b->collision, b->storage, b->table, b->item_lat,
+                                              b->items, src, dst, grid, b->block,
+                                              b->blocks_per_sm > 0, s);
         if (rc) return rc;
     }
     return LBM_OK;
@@ -117,16 +120,27 @@ int lbm_batch_create(const LbmDesc* lattices, int count, LbmBatch** out) {
     }
     b->elements = base;
     b->items = int(items);
+    std::vector<uint16_t> owner(size_t(b->items));
+    for (int l = 0; l < count; ++l) {
+        const int end = l + 1 < count ? host[l + 1].item0 : b->items;
+        for (int k = host[l].item0; k < end; ++k) owner[size_t(k)] = uint16_t(l);
+    }
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->table),
                                sizeof(lbm::BatchLattice) * count);
     if (e == cudaSuccess)
+        e = cudaMalloc(reinterpret_cast<void**>(&b->item_lat), sizeof(uint16_t) * owner.size());
+    if (e == cudaSuccess)
         e = cudaMemcpy(b->table, host.data(), sizeof(lbm::BatchLattice) * count,
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->item_lat, owner.data(), sizeof(uint16_t) * owner.size(),
                        cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         if (b->table) cudaFree(b->table);
+        if (b->item_lat) cudaFree(b->item_lat);
         delete b;
         return int(e);
     }
@@ -138,6 +152,7 @@ int lbm_batch_destroy(LbmBatch* b) {
     if (b == nullptr) return LBM_E_HANDLE;
     drop_graph(b);
     if (b->table) cudaFree(b->table);
+    if (b->item_lat) cudaFree(b->item_lat);
     delete b;
     return LBM_OK;
 }
@@ -161,7 +176,7 @@ int lbm_batch_offsets(const LbmBatch* b, int64_t* bases) {
 int lbm_batch_set_launch(LbmBatch* b, int block, int blocks_per_sm) {
     if (b == nullptr) return LBM_E_HANDLE;
     if (block != 64 && block != 128 && block != 256) return LBM_E_ARG;
-    if (blocks_per_sm < 1 || blocks_per_sm > 64) return LBM_E_ARG;
+    if (blocks_per_sm < 0 || blocks_per_sm > 64) return LBM_E_ARG;
     if (block != b->block || blocks_per_sm != b->blocks_per_sm) drop_graph(b);
     b->block = block;
     b->blocks_per_sm = blocks_per_sm;

@@ -43,10 +43,12 @@ struct BatchLattice {
     float ulid, r0, r1, r2, r3;
 };
 
-// One step of every lattice of a batch (D2Q9 pull, two buffers).
-int launch_batch_d2q9(int collision, int storage, const BatchLattice* lats, int nlat,
-                      int items, const void* src, void* dst, int grid, int block,
-                      cudaStream_t s);
+// One step of every lattice of a batch (D2Q9 pull, two buffers). item_lat[k] is the lattice
+// of work item k; persist selects the grid-stride kernel (grid smaller than the item count)
+// over the one-item-per-warp kernel (grid covering every item).
+int launch_batch_d2q9(int collision, int storage, const BatchLattice* lats,
+                      const uint16_t* item_lat, int items, const void* src, void* dst, int grid,
+                      int block, bool persist, cudaStream_t s);
 
 // Per-launch configuration of the TMA-staged kernels (see lbm_set_staged_config).
 struct StagedTune {
