@@ -1,4 +1,5 @@
-// D3Q19 specialised kernels: TMA-staged pull for AB and AA-odd, vector AA-even.
+// D3Q19 specialised kernels: register row kernels for the AB pull and the AA-odd step (the
+// default), the TMA-staged kernel for both with LBM_FLAG_STAGED, vector AA-even.
 #include "codec.cuh"
 #include "collide.cuh"
 #include "dispatch.cuh"
@@ -18,7 +19,8 @@ int go(const StepParams& P, const void* src, void* dst, int pattern, cudaStream_
         if (staged) return go_staged<L, STORE, COLL, FORCE, LBM_PATTERN_AB>(P, src, dst, s);
         return rows3d::go_ab<STORE, COLL, FORCE>(P, src, dst, s);
     }
-    return go_staged<L, STORE, COLL, FORCE, LBM_PATTERN_AA_ODD>(P, dst, dst, s);
+    if (staged) return go_staged<L, STORE, COLL, FORCE, LBM_PATTERN_AA_ODD>(P, dst, dst, s);
+    return rows3d::go_aa_odd<STORE, COLL, FORCE>(P, dst, s);
 }
 
 template <int STORE, int COLL>

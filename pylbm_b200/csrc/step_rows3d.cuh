@@ -122,9 +122,12 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
     }
 }
 
+// Collide the V nodes of the lane in place. With LIDS, lid[i] is added to the pulled value of
+// direction i and sub[i] is subtracted from its post-collision value (the AA-odd push into
+// the lid).
 template <int STORE, int COLL, bool FORCE, bool LIDS>
 __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19],
-                                             const float (&lid)[19]) {
+                                             const float (&lid)[19], const float (&sub)[19]) {
     using T = VT<STORE>;
     constexpr int V = T::V;
     const float F[3] = {P.F[0], P.F[1], P.F[2]};
@@ -139,7 +142,7 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19]
             }
             collide<L, COLL, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
-            for (int i = 0; i < 19; ++i) put<V>(v[i], k, T::b(f[i]));
+            for (int i = 0; i < 19; ++i) put<V>(v[i], k, T::b(LIDS ? sub_lid(f[i], sub[i]) : f[i]));
         }
     } else {
         // 16-bit: two nodes per word, packed conversions, the two nodes collided one after the
@@ -159,7 +162,10 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19]
             collide<L, COLL, Codec<STORE>::shifted, FORCE, true>(f0, F, P.r0, P.r1, P.r2, P.r3);
             collide<L, COLL, Codec<STORE>::shifted, FORCE, true>(f1, F, P.r0, P.r1, P.r2, P.r3);
 #pragma unroll
-            for (int i = 0; i < 19; ++i) set_word(v[i], jw, pack2<STORE>(f0[i], f1[i]));
+            for (int i = 0; i < 19; ++i)
+                set_word(v[i], jw, LIDS ? pack2<STORE>(sub_lid(f0[i], sub[i]),
+                                                       sub_lid(f1[i], sub[i]))
+                                        : pack2<STORE>(f0[i], f1[i]));
         }
     }
 }
@@ -171,7 +177,8 @@ __device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<ST
     float lid[19];
     pull_rows<STORE, false, true, EDGE>(P, A, l, v, lid);
     if (!l.active) return;
-    collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid);
+    const float zero[19] = {};
+    collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid, zero);
     const int n0 = (l.y + P.n[1] * l.z) * P.n[0] + l.x0;
 #pragma unroll
     for (int i = 0; i < 19; ++i) st_cs(B + i * P.N + n0, v[i]);
@@ -188,6 +195,83 @@ k_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
     else ab_row<STORE, COLL, FORCE, false>(P, A, B, l);
 }
 
+// AA odd step in place (the D2Q9 design of step_d2q9.cu over rows (y, z)): pull from the
+// swapped slots A[opp(i), x - c_i] (bounce-back: A[i, x]), collide, push p_i to
+// A[i, x + c_i] or, behind a wall, to the node's own slot A[opp(i), x] minus the lid term.
+// Every slot is read and written by one node only (slot (i, x + c_i) belongs to node x), so
+// a lane stores an aligned vector only where all its elements belong to nodes of its own
+// warp, which loaded before any lane of the warp stores; the warp-edge lanes store the
+// slots of their own nodes one element at a time.
+template <int STORE, int COLL, bool FORCE, bool EDGE>
+__device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STORE>::E* A,
+                                           const Lane3& l) {
+    using E = typename VT<STORE>::E;
+    constexpr int V = VT<STORE>::V;
+    const int nx = P.n[0], N = P.N;
+    uint4 v[19];
+    float lid[19], sub[19];
+    pull_rows<STORE, true, false, EDGE>(P, A, l, v, lid);
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {  // pushes bouncing off the lid carry its term, negated
+        bool wall, top;
+        src_row<EDGE>(P, l.y, l.z, -L::cy(i), -L::cz(i), wall, top);
+        sub[i] = (wall && top && L::cx(i) != 0) ? lid_term<L>(i, P.ulid) : 0.0f;
+    }
+    if (l.active) collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid, sub);
+    const int own_row = l.y + P.n[1] * l.z;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        const int cx = L::cx(i);
+        bool wall, top;
+        const int r = src_row<EDGE>(P, l.y, l.z, -L::cy(i), -L::cz(i), wall, top);
+        E* plane = A + i * N + r * nx;
+        E* bb = A + L::opp(i) * N + own_row * nx;  // own row, opposite slot
+        if (wall) {
+            if (l.active) st_plain(bb + l.x0, v[i]);
+            continue;
+        }
+        if (cx == 0) {
+            if (l.active) st_plain(plane + l.x0, v[i]);
+        } else if (cx == 1) {
+            const uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
+            if (!l.active) continue;
+            if (!l.first) {
+                st_plain(plane + l.x0, shift_up<V>(v[i], up));
+            } else {
+#pragma unroll
+                for (int k = 0; k < V - 1; ++k) st1(plane + l.x0 + 1 + k, elem<V>(v[i], k));
+            }
+            if (l.last) {
+                E* dst = l.x0 + V < nx ? plane + l.x0 + V : (P.per[0] ? plane : bb + nx - 1);
+                st1(dst, elem<V>(v[i], V - 1));
+            }
+        } else {
+            const uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
+            if (!l.active) continue;
+            if (!l.last) {
+                st_plain(plane + l.x0, shift_down<V>(v[i], dn));
+            } else {
+#pragma unroll
+                for (int k = 1; k < V; ++k) st1(plane + l.x0 + k - 1, elem<V>(v[i], k));
+            }
+            if (l.first) {
+                E* dst = l.x0 > 0 ? plane + l.x0 - 1 : (P.per[0] ? plane + nx - 1 : bb);
+                st1(dst, elem<V>(v[i], 0));
+            }
+        }
+    }
+}
+
+template <int STORE, int COLL, bool FORCE>
+__global__ void __launch_bounds__(kThreads, 3)
+k_aa_odd(const StepParams P, void* Av) {
+    using E = typename VT<STORE>::E;
+    E* A = static_cast<E*>(Av);
+    const Lane3 l = lane_of<VT<STORE>::V>(P);
+    if (edge_row(P, l.y, l.z)) aa_odd_row<STORE, COLL, FORCE, true>(P, A, l);
+    else aa_odd_row<STORE, COLL, FORCE, false>(P, A, l);
+}
+
 // Block shape (lanes along x, rows) for rows of nx nodes.
 inline dim3 block_for_rows(int nx, int V) {
     int lanes = (nx / V + 31) / 32 * 32;
@@ -202,6 +286,16 @@ int go_ab(const StepParams& P, const void* src, void* dst, cudaStream_t s) {
     const dim3 grid((P.n[0] / V + block.x - 1) / block.x, (P.n[1] + block.y - 1) / block.y,
                     P.n[2]);
     k_ab<STORE, COLL, FORCE><<<grid, block, 0, s>>>(P, src, dst);
+    return int(cudaGetLastError());
+}
+
+template <int STORE, int COLL, bool FORCE>
+int go_aa_odd(const StepParams& P, void* buf, cudaStream_t s) {
+    constexpr int V = VT<STORE>::V;
+    const dim3 block = block_for_rows(P.n[0], V);
+    const dim3 grid((P.n[0] / V + block.x - 1) / block.x, (P.n[1] + block.y - 1) / block.y,
+                    P.n[2]);
+    k_aa_odd<STORE, COLL, FORCE><<<grid, block, 0, s>>>(P, buf);
     return int(cudaGetLastError());
 }
 
