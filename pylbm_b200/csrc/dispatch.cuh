@@ -40,15 +40,16 @@ struct BatchLattice {
     int periodic_mask;
     int item0;          // first warp work item of the lattice
     int segs;           // V-node vectors per row (a work item is 32 consecutive vectors)
+    int y0, xv0;        // per-item copies: row and vector offset of the item's first vector
     float ulid, r0, r1, r2, r3;
 };
 
-// One step of every lattice of a batch (D2Q9 pull, two buffers). item_lat[k] is the lattice
-// of work item k; persist selects the grid-stride kernel (grid smaller than the item count)
-// over the one-item-per-warp kernel (grid covering every item).
-int launch_batch_d2q9(int collision, int storage, const BatchLattice* lats,
-                      const uint16_t* item_lat, int items, const void* src, void* dst, int grid,
-                      int block, bool persist, cudaStream_t s);
+// One step of every lattice of a batch (D2Q9 pull, two buffers). item_tab[k] holds the
+// parameters of the lattice of work item k; persist selects the grid-stride kernel (grid
+// smaller than the item count) over the one-item-per-warp kernel (grid covering every item).
+int launch_batch_d2q9(int collision, int storage, const BatchLattice* item_tab, int items,
+                      const void* src, void* dst, int grid, int block, bool persist,
+                      cudaStream_t s);
 
 // Per-launch configuration of the TMA-staged kernels (see lbm_set_staged_config).
 struct StagedTune {

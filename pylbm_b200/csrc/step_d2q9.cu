@@ -372,17 +372,17 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 // One launch advances every lattice of a batch by one step. Each lattice's rows are laid end
 // to end as one sequence of V-node vectors (nx / V per row); a work item is 32 consecutive
 // vectors, one per lane, so rows narrower than a warp do not leave lanes idle. Lattice l owns
-// items [item0_l, item0_l + ceil(nx ny / V / 32)). A warp reads its lattice from a per-item
-// table (uniform per warp) and runs the single-lattice row code on that lattice's slice of
-// the buffers: the lane at a row start, or at the warp start, takes its
+// items [item0_l, item0_l + ceil(nx ny / V / 32)). A warp reads its lattice's parameters from
+// a per-item copy (one uniform load, no lattice lookup before it) and runs the single-lattice
+// row code on that lattice's slice of the buffers: the lane at a row start, or at the warp start, takes its
 // x-halo from memory instead of from its neighbour lane. A warp touching a row next to a y
 // wall takes the general (wall and lid) path as a whole. PERSIST: a grid of a tuned size whose
 // warps stride over the items; otherwise one item per warp (no loop state to keep, which
 // leaves more registers to the collision).
 template <int STORE, int COLL, bool PERSIST>
 __global__ void __launch_bounds__(256)
-k_d2q9_batch_ab(const BatchLattice* __restrict__ lats, const uint16_t* __restrict__ item_lat,
-                int items, const void* __restrict__ Av, void* __restrict__ Bv) {
+k_d2q9_batch_ab(const BatchLattice* __restrict__ item_tab, int items,
+                const void* __restrict__ Av, void* __restrict__ Bv) {
     using E = typename VT<STORE>::E;
     constexpr int V = VT<STORE>::V;
     const E* __restrict__ A = static_cast<const E*>(Av);
@@ -391,7 +391,7 @@ k_d2q9_batch_ab(const BatchLattice* __restrict__ lats, const uint16_t* __restric
     const int stride = PERSIST ? (gridDim.x * blockDim.x) >> 5 : items;
     for (int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < items;
          item += stride) {
-        const BatchLattice& bl = lats[__ldg(item_lat + item)];
+        const BatchLattice& bl = item_tab[item];
         const int local = item - __ldg(&bl.item0);
         const int vrow = __ldg(&bl.segs);  // vectors per row
         StepParams P;
@@ -417,8 +417,14 @@ k_d2q9_batch_ab(const BatchLattice* __restrict__ lats, const uint16_t* __restric
         Lane l;
         l.lane = lane;
         l.active = vidx < nvec;
-        l.y = l.active ? vidx / vrow : 0;
-        l.x0 = l.active ? (vidx - l.y * vrow) * V : 0;
+        // row of the lane's vector: from the item's first row, a few whole rows further
+        int xv = __ldg(&bl.xv0) + lane, y = __ldg(&bl.y0);
+        while (xv >= vrow) {
+            xv -= vrow;
+            ++y;
+        }
+        l.y = l.active ? y : 0;
+        l.x0 = l.active ? xv * V : 0;
         l.first = lane == 0 || l.x0 == 0;
         l.last = l.active && (lane == 31 || l.x0 + V >= P.n[0] || vidx + 1 >= nvec);
         const long long base = __ldg(&bl.base);
@@ -429,20 +435,20 @@ k_d2q9_batch_ab(const BatchLattice* __restrict__ lats, const uint16_t* __restric
 }
 
 template <int STORE, bool PERSIST>
-int batch_go(int collision, const BatchLattice* lats, const uint16_t* item_lat, int items,
-             const void* src, void* dst, int grid, int block, cudaStream_t s) {
+int batch_go(int collision, const BatchLattice* item_tab, int items, const void* src,
+             void* dst, int grid, int block, cudaStream_t s) {
     switch (collision) {
         case LBM_BGK:
             k_d2q9_batch_ab<STORE, LBM_BGK, PERSIST>
-                <<<grid, block, 0, s>>>(lats, item_lat, items, src, dst);
+                <<<grid, block, 0, s>>>(item_tab, items, src, dst);
             break;
         case LBM_TRT:
             k_d2q9_batch_ab<STORE, LBM_TRT, PERSIST>
-                <<<grid, block, 0, s>>>(lats, item_lat, items, src, dst);
+                <<<grid, block, 0, s>>>(item_tab, items, src, dst);
             break;
         case LBM_MRT:
             k_d2q9_batch_ab<STORE, LBM_MRT, PERSIST>
-                <<<grid, block, 0, s>>>(lats, item_lat, items, src, dst);
+                <<<grid, block, 0, s>>>(item_tab, items, src, dst);
             break;
         default:
             return LBM_E_COLLISION;
@@ -451,31 +457,29 @@ int batch_go(int collision, const BatchLattice* lats, const uint16_t* item_lat, 
 }
 
 template <int STORE>
-int batch_go_p(int collision, const BatchLattice* lats, const uint16_t* item_lat, int items,
-               const void* src, void* dst, int grid, int block, bool persist, cudaStream_t s) {
-    return persist ? batch_go<STORE, true>(collision, lats, item_lat, items, src, dst, grid,
-                                           block, s)
-                   : batch_go<STORE, false>(collision, lats, item_lat, items, src, dst, grid,
-                                            block, s);
+int batch_go_p(int collision, const BatchLattice* item_tab, int items, const void* src,
+               void* dst, int grid, int block, bool persist, cudaStream_t s) {
+    return persist ? batch_go<STORE, true>(collision, item_tab, items, src, dst, grid, block, s)
+                   : batch_go<STORE, false>(collision, item_tab, items, src, dst, grid, block, s);
 }
 
 }  // namespace
 
-int launch_batch_d2q9(int collision, int storage, const BatchLattice* lats,
-                      const uint16_t* item_lat, int items, const void* src, void* dst, int grid,
-                      int block, bool persist, cudaStream_t s) {
+int launch_batch_d2q9(int collision, int storage, const BatchLattice* item_tab, int items,
+                      const void* src, void* dst, int grid, int block, bool persist,
+                      cudaStream_t s) {
     switch (storage) {
         case LBM_STORE_F32:
-            return batch_go_p<LBM_STORE_F32>(collision, lats, item_lat, items, src, dst, grid,
+            return batch_go_p<LBM_STORE_F32>(collision, item_tab, items, src, dst, grid,
                                              block, persist, s);
         case LBM_STORE_F32_SHIFTED:
-            return batch_go_p<LBM_STORE_F32_SHIFTED>(collision, lats, item_lat, items, src, dst,
-                                                     grid, block, persist, s);
+            return batch_go_p<LBM_STORE_F32_SHIFTED>(collision, item_tab, items, src, dst, grid,
+                                                     block, persist, s);
         case LBM_STORE_F16:
-            return batch_go_p<LBM_STORE_F16>(collision, lats, item_lat, items, src, dst, grid,
+            return batch_go_p<LBM_STORE_F16>(collision, item_tab, items, src, dst, grid,
                                              block, persist, s);
         case LBM_STORE_BF16:
-            return batch_go_p<LBM_STORE_BF16>(collision, lats, item_lat, items, src, dst, grid,
+            return batch_go_p<LBM_STORE_BF16>(collision, item_tab, items, src, dst, grid,
                                               block, persist, s);
     }
     return LBM_E_STORAGE;
