@@ -379,8 +379,13 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 // wall takes the general (wall and lid) path as a whole. PERSIST: a grid of a tuned size whose
 // warps stride over the items; otherwise one item per warp (no loop state to keep, which
 // leaves more registers to the collision).
+//
+// 16-bit MRT batches are capped at 80 registers (3 blocks of 256 threads per SM; 12 bytes of
+// spills): latency-bound at 96 registers and 20 warps per SM, they measured 152K instead of
+// 146K MLUPS on the 64-cavity workload at 24 warps. The packed BGK / TRT batches spill too
+// much under that cap.
 template <int STORE, int COLL, bool PERSIST>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, (VT<STORE>::V == 8 && COLL == LBM_MRT) ? 3 : 1)
 k_d2q9_batch_ab(const BatchLattice* __restrict__ item_tab, int items,
                 const void* __restrict__ Av, void* __restrict__ Bv) {
     using E = typename VT<STORE>::E;

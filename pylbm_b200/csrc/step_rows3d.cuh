@@ -184,8 +184,12 @@ __device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<ST
     for (int i = 0; i < 19; ++i) st_cs(B + i * P.N + n0, v[i]);
 }
 
+// 16-bit without a body force: capped at 128 registers (4 blocks per SM), which the compiler
+// meets without spills; left free it takes ~158 and 3 blocks, and this latency-bound kernel
+// measured 79.5K instead of 72.5K MLUPS (256^3 TRT fp16). The forced variants would spill
+// several hundred bytes under the cap.
 template <int STORE, int COLL, bool FORCE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, (VT<STORE>::V == 8 && !FORCE) ? 4 : 1)
 k_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
     using E = typename VT<STORE>::E;
     const E* __restrict__ A = static_cast<const E*>(Av);
