@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 1
+#define LBM_ABI_VERSION 2
 
 /* lattices */
 #define LBM_D2Q9 0
@@ -68,6 +68,7 @@ extern "C" {
 #define LBM_E_HANDLE -14     /* unknown or destroyed handle */
 #define LBM_E_ARG -15        /* any other invalid argument */
 #define LBM_E_SIZE -16       /* problem larger than a fixed capacity */
+#define LBM_E_INOUT -17      /* inlet / outlet without D2Q9, x walls and the two-buffer pull */
 
 /* Problem descriptor: the compile-time #defines and runtime scalars of pylbm's fused kernel
  * (backends/cupy_backend.py:51-70 header, backends/_fused.py:129-136 scalar_args) as one POD.
@@ -91,7 +92,11 @@ typedef struct LbmDesc {
     int64_t mx_stride;          /* doubles between the slots of consecutive steps in
                                    lbm_advance (0 = every step adds into the same slot) */
     int32_t flags;              /* LBM_FLAG_* bits, 0 by default */
-    int32_t reserved;
+    int32_t outlet;             /* 1: pressure outlet on the right boundary (pylbm's
+                                   Problem.outlet, core.py:130-148); D2Q9, x walls, AB only */
+    const float* inlet_u;       /* velocity inlet on the left wall (Problem.inlet,
+                                   core.py:67-78,116-117): u_x per row y, ny floats on the
+                                   device; D2Q9, x walls, AB only */
 } LbmDesc;
 
 /* descriptor flags */

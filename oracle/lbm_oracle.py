@@ -93,6 +93,8 @@ class Case:
     solid: Any = None        # bool (ny, nx) / (nz, ny, nx)
     force_field: Any = None  # (d, *array_shape) float64, added to ``force``
     extra: dict = field(default_factory=dict)
+    inlet: Any = None        # u_x(y) of the velocity inlet on the left wall, (ny,), 2D
+    outlet: bool = False     # pressure outlet (rho = 1) on the right boundary, 2D
 
     def __post_init__(self) -> None:
         self.shape = tuple(int(s) for s in self.shape)
@@ -106,7 +108,8 @@ class Case:
     @classmethod
     def from_problem(cls, p: Any, force_field: Any = None) -> Case:
         return cls(p.shape, p.tau, p.collision, p.periodic, p.u_lid, p.force, p.magic,
-                   p.s_e, p.s_eps, getattr(p, "solid", None), force_field)
+                   p.s_e, p.s_eps, getattr(p, "solid", None), force_field,
+                   inlet=getattr(p, "inlet", None), outlet=bool(getattr(p, "outlet", False)))
 
     @property
     def dim(self) -> int:
@@ -207,14 +210,44 @@ def stream(f: Any, case: Case, xp: Any = np, solid_src: list | None = None) -> l
             ca = lat.c[i][a]
             if ca == 1:  # the source lies behind the low wall
                 fc = _face(d, a, 0)
-                out[i][fc] = f[opp[i]][fc]
+                val = f[opp[i]][fc]
+                if a == 0 and case.inlet is not None:  # moving-wall inlet (core.py:67-78,116-117)
+                    val = val + 6.0 * lat.w[i] * lat.c[i][0] * _as(case.inlet, f, X)
+                out[i][fc] = val
             elif ca == -1:  # the source lies behind the high wall
                 fc = _face(d, a, -1)
                 val = f[opp[i]][fc]
                 if top and case.u_lid != 0.0 and lat.c[i][0] != 0:
                     val = val + 6.0 * lat.w[i] * lat.c[i][0] * case.u_lid
                 out[i][fc] = val
+    if case.outlet:
+        _outlet(out, f, case)
     return out
+
+
+def _as(a: Any, like: Any, X: Any) -> Any:
+    """``a`` as an array of the backend of ``like`` (numpy or torch)."""
+    if X.torch:
+        return X.xp.as_tensor(np.asarray(a), dtype=like.dtype)
+    return np.asarray(a, dtype=np.float64)
+
+
+def _outlet(out: list, f: Any, case: Case) -> None:
+    """Pressure outlet on the right boundary (core.py:130-148, D2Q9): the populations that
+    enter from the right (c_x = -1) are the equilibrium at rho = 1 with the velocity of the
+    neighbouring column, taken from the stored post-collision state."""
+    lat = case.lat
+    col = [f[i][..., -2] for i in range(lat.q)]
+    rho = col[0]
+    for i in range(1, lat.q):
+        rho = rho + col[i]
+    ux = (col[1] - col[3] + col[5] - col[6] - col[7] + col[8]) / rho
+    uy = (col[2] - col[4] + col[5] + col[6] - col[7] - col[8]) / rho
+    usq = ux * ux + uy * uy
+    for i in range(lat.q):
+        if lat.c[i][0] == -1:
+            cu = lat.c[i][0] * ux + lat.c[i][1] * uy
+            out[i][..., -1] = lat.w[i] * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq)
 
 
 def moments(f: list, case: Case) -> tuple:

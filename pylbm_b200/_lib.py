@@ -45,7 +45,8 @@ class LbmDesc(ctypes.Structure):
         ("mx_force", ctypes.c_void_p),
         ("mx_stride", ctypes.c_int64),
         ("flags", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("outlet", ctypes.c_int32),
+        ("inlet_u", ctypes.c_void_p),
     ]
 
 
@@ -103,7 +104,7 @@ def load() -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = res
-    if lib.lbm_abi_version() != 1:
+    if lib.lbm_abi_version() != 2:
         raise RuntimeError("libpylbm_b200 ABI version mismatch")
     _LIB = lib
     return lib

@@ -109,7 +109,12 @@ class B200Fused:
     @classmethod
     def supports(cls, problem: Any) -> tuple[bool, str]:
         if getattr(problem, "inlet", None) is not None or getattr(problem, "outlet", False):
-            return False, "inlet / outlet boundaries are not implemented in the fused kernels"
+            if cls.aa:
+                return False, "inlet / outlet need the two-buffer variant (fused, fused-fp16, ...)"
+            if problem.dim != 2 or problem.periodic[0]:
+                return False, "inlet / outlet are defined for D2Q9 with walls on the x axis"
+            if problem.shape[0] < 3:
+                return False, "inlet / outlet need nx >= 3"
         if getattr(problem, "solid", None) is not None and cls.aa:
             return False, "solid obstacles need the two-buffer variant (fused, fused-fp16, ...)"
         if problem.lattice.name not in cls.lattices:
@@ -152,6 +157,14 @@ class B200Fused:
             self._keep.append(bits)
             self.solid_mask = bits
             self.desc.solid_bits = bits.data_ptr()
+        if getattr(problem, "inlet", None) is not None:  # u_x(y) on the left wall
+            uin = torch.as_tensor(np.asarray(problem.inlet, dtype=np.float32).reshape(-1),
+                                  device=self.dev).contiguous()
+            if uin.numel() != problem.shape[1]:
+                raise ValueError(f"inlet must hold ny = {problem.shape[1]} values")
+            self._keep.append(uin)
+            self.desc.inlet_u = uin.data_ptr()
+        self.desc.outlet = int(bool(getattr(problem, "outlet", False)))
         if force_field is not None:
             self.set_force_field(force_field)
         _lib.call("lbm_validate", ctypes.byref(self.desc))

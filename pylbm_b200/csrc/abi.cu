@@ -68,6 +68,7 @@ int check_pattern(const LbmDesc& d, const void* src, const void* dst, int patter
     // each memory slot owned by one node once a link is blocked on one side only
     if (pattern != LBM_PATTERN_AB && (d.solid_bits != nullptr || d.mx_force != nullptr))
         return LBM_E_ARG;
+    if (pattern != LBM_PATTERN_AB && (d.inlet_u != nullptr || d.outlet)) return LBM_E_INOUT;
     return LBM_OK;
 }
 
@@ -136,6 +137,8 @@ const char* lbm_error_string(int code) {
         case LBM_E_HANDLE: return "unknown or destroyed handle";
         case LBM_E_ARG: return "invalid argument";
         case LBM_E_SIZE: return "problem exceeds a fixed capacity";
+        case LBM_E_INOUT:
+            return "inlet and outlet boundaries need D2Q9, walls on the x axis and the AB pattern";
     }
     if (code > 0) return cudaGetErrorString(static_cast<cudaError_t>(code));
     return "unknown error";
@@ -187,6 +190,11 @@ int lbm_validate(const LbmDesc* d) {
         if (!d->solid_bits) return LBM_E_ARG;
     }
     if (d->mx_stride < 0) return LBM_E_ARG;
+    if (d->outlet != 0 && d->outlet != 1) return LBM_E_ARG;
+    if (d->inlet_u || d->outlet) {
+        if (d->lattice != LBM_D2Q9 || (d->periodic_mask & 1) || d->nx < 3) return LBM_E_INOUT;
+        if (d->inlet_u && !aligned(d->inlet_u, 4)) return LBM_E_ALIGN;
+    }
     return LBM_OK;
 }
 

@@ -88,7 +88,8 @@ int lbm_batch_create(const LbmDesc* lattices, int count, LbmBatch** out) {
         if (!rc && (d.lattice != LBM_D2Q9 || d.collision != d0.collision ||
                     d.storage != d0.storage || d.collision == LBM_STREAM_ONLY))
             rc = LBM_E_ARG;
-        if (!rc && (d.solid_bits || d.force_field || d.mx_force || d.fx != 0.0f || d.fy != 0.0f))
+        if (!rc && (d.solid_bits || d.force_field || d.mx_force || d.fx != 0.0f || d.fy != 0.0f ||
+                    d.inlet_u || d.outlet))
             rc = LBM_E_ARG;  // batches are plain boxes
         if (!rc && d.nx % V != 0) rc = LBM_E_SHAPE;
         if (rc) {

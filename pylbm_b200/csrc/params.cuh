@@ -19,6 +19,8 @@ struct StepParams {
     const uint32_t* solid;  // optional 1-bit-per-node solid mask
     const float* field;     // optional per-node force (d, N)
     double* mx;             // optional momentum-exchange accumulator [d]
+    const float* inlet;     // optional velocity inlet u_x(y) on the left wall (D2Q9)
+    int outlet;             // 1: pressure outlet on the right boundary (D2Q9)
 };
 
 inline StepParams make_params(const LbmDesc& d) {
@@ -40,6 +42,8 @@ inline StepParams make_params(const LbmDesc& d) {
     p.solid = d.solid_bits;
     p.field = d.force_field;
     p.mx = d.mx_force;
+    p.inlet = d.inlet_u;
+    p.outlet = d.outlet;
     return p;
 }
 

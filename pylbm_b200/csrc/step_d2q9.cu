@@ -417,6 +417,8 @@ k_d2q9_batch_ab(const BatchLattice* __restrict__ item_tab, int items,
         P.solid = nullptr;
         P.field = nullptr;
         P.mx = nullptr;
+        P.inlet = nullptr;
+        P.outlet = 0;
         const int vidx = local * 32 + lane;
         const int nvec = vrow * P.n[1];
         Lane l;
@@ -493,7 +495,7 @@ int launch_batch_d2q9(int collision, int storage, const BatchLattice* item_tab, 
 int launch_fast_d2q9(const LbmDesc& d, const void* src, void* dst, int pattern,
                      cudaStream_t s) {
     // the vector kernels cover box problems whose rows split into whole 16-byte vectors
-    if (d.solid_bits || d.force_field || d.mx_force) return 1;
+    if (d.solid_bits || d.force_field || d.mx_force || d.inlet_u || d.outlet) return 1;
     const int V = (d.storage == LBM_STORE_F16 || d.storage == LBM_STORE_BF16) ? 8 : 4;
     if (d.nx % V != 0) return 1;
     if (!aligned16(src) || !aligned16(dst)) return 1;

@@ -57,7 +57,7 @@ int launch_staged_timeout_probe(const LbmDesc& d, void* buf, unsigned long long 
 
 int launch_fast_d3q19(const LbmDesc& d, const void* src, void* dst, int pattern,
                       cudaStream_t s) {
-    if (d.solid_bits || d.force_field || d.mx_force) return 1;
+    if (d.solid_bits || d.force_field || d.mx_force || d.inlet_u || d.outlet) return 1;
     const int V = (d.storage == LBM_STORE_F16 || d.storage == LBM_STORE_BF16) ? 8 : 4;
     if (d.nx % V != 0) return 1;
     if (!aligned16(src) || !aligned16(dst)) return 1;

@@ -67,6 +67,50 @@ __device__ __forceinline__ int wrapped(const StepParams& P, const int (&crd)[3],
     return idx;
 }
 
+// Velocity inlet on the left wall (core.py:67-78,116-117): a pull of direction i (c_ix = +1)
+// at x = 0 bounces back with Ladd's term for the wall speed u_in(y), 6 w_i c_ix u_in(y),
+// unless the source also lies behind a y wall, whose rule comes later in pylbm's axis loop
+// and wins at the corners.
+template <class L>
+__device__ __forceinline__ void apply_inlet(const StepParams& P, int y, float (&f)[L::Q]) {
+    const float uin = __ldg(P.inlet + y);
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        if (L::cx(i) != 1) continue;
+        const int ys = y - L::cy(i);
+        if (!P.per[1] && (ys < 0 || ys >= P.n[1])) continue;
+        f[i] = add_lid(f[i], __fmul_rn(6.0f * L::w(i) * float(L::cx(i)), uin));
+    }
+}
+
+// Pressure outlet on the right boundary (core.py:130-148), applied after every other rule:
+// the pulls with c_ix = -1 at x = nx - 1 take the equilibrium at rho = 1 and the velocity of
+// the neighbouring column x = nx - 2 of the stored (pre-streaming) state, in pylbm's order of
+// operations; shifted storages hold that equilibrium minus w_i.
+template <class L, class C>
+__device__ __forceinline__ void apply_outlet(const StepParams& P,
+                                             const typename C::T* __restrict__ A, int n,
+                                             float (&f)[L::Q]) {
+    static_assert(L::Q == 9, "the outlet is defined for D2Q9");
+    float col[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) col[i] = C::ld(A[i * P.N + n - 1]);
+    float rho = col[0];
+#pragma unroll
+    for (int i = 1; i < 9; ++i) rho = rho + col[i];
+    if (C::shifted) rho = 1.0f + rho;
+    const float ux = (col[1] - col[3] + col[5] - col[6] - col[7] + col[8]) / rho;
+    const float uy = (col[2] - col[4] + col[5] + col[6] - col[7] - col[8]) / rho;
+    const float usq = ux * ux + uy * uy;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        if (L::cx(i) != -1) continue;
+        const float cu = float(L::cx(i)) * ux + float(L::cy(i)) * uy;
+        const float dev = 3.0f * cu + 4.5f * cu * cu - 1.5f * usq;
+        f[i] = C::shifted ? L::w(i) * dev : L::w(i) * (1.0f + dev);
+    }
+}
+
 template <class L, int COLL, int STORE, int PATTERN, bool FORCE>
 __global__ void __launch_bounds__(128)
 k_step_generic(const StepParams P, const typename Codec<STORE>::T* A,
@@ -102,6 +146,10 @@ k_step_generic(const StepParams P, const typename Codec<STORE>::T* A,
             }
             f[i] = C::ld(A[idx]);
             if (top && L::cx(i) != 0) f[i] = add_lid(f[i], lid_term<L>(i, P.ulid));
+        }
+        if constexpr (L::D == 2 && PATTERN == LBM_PATTERN_AB) {  // open boundaries
+            if (P.inlet != nullptr && x == 0) apply_inlet<L>(P, y, f);
+            if (P.outlet && x == P.n[0] - 1) apply_outlet<L, C>(P, A, n, f);
         }
         // ------------------------------------------------------------ collide
         float F[3] = {P.F[0], P.F[1], P.F[2]};

@@ -17,7 +17,10 @@ the rest equilibrium, the step count and pylbm's float64 NumPy result:
                 lid off, and to zeros with the lid on (the construction of
                 torch_backend.py:80-101);
 * ``dJdg``      central finite difference, on pylbm's NumPy solver, of the mean x drag over
-                steps t0..T with respect to the uniform body force g_x (small channel + disc).
+                steps t0..T with respect to the uniform body force g_x (small channel + disc);
+* ``inout_*``   velocity inlet and pressure outlet (core.py:67-78,116-117,130-148): pylbm's
+                Schaefer-Turek channel at 4 nodes per diameter (karman.py:21-42) with the drag
+                after every step, and a BGK channel from a random state.
 """
 
 from __future__ import annotations
@@ -136,6 +139,33 @@ def solid_cases() -> None:
              f=s.populations(), force_hist=np.array(hist))
 
 
+def inout_cases() -> None:
+    from pylbm.validation.karman import schafer_turek_problem
+
+    p = schafer_turek_problem(d=4, u_mean=0.05, collision="trt")
+    masks, c = _force_masks(p)
+    mk = np.stack(masks).astype(float)
+    s = NumpySolver(p)
+    f0 = s.populations()
+    hist = []
+    for _ in range(60):
+        s.step(1)
+        per_dir = (s.populations() * mk).sum(axis=(1, 2))
+        hist.append(2.0 * (per_dir[:, None] * c).sum(0))
+    save("inout_karman_trt", params=json.dumps(params_of(p)), steps=60, solid=p.solid,
+         inlet=p.inlet, outlet=True, f0=f0, f=s.populations(), force_hist=np.array(hist))
+    nx, ny = 40, 12
+    yy = np.arange(ny) + 0.5
+    inlet = 4.0 * 0.06 * yy * (ny - yy) / ny**2
+    p = Problem((nx, ny), tau=0.62, periodic=(False, False), inlet=inlet, outlet=True)
+    f0 = random_state(p, 21, amp=0.03)
+    s = NumpySolver(p)
+    s.set_populations(f0)
+    s.step(50)
+    save("inout_channel_bgk", params=json.dumps(params_of(p)), steps=50, inlet=inlet,
+         outlet=True, f0=f0, f=s.populations())
+
+
 def tag_maps() -> None:
     cases = {
         "tags_cavity2d": Problem((7, 5), u_lid=0.1),
@@ -191,3 +221,4 @@ if __name__ == "__main__":
     solid_cases()
     tag_maps()
     drag_fd()
+    inout_cases()

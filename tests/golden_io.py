@@ -22,7 +22,8 @@ def load(name: str) -> dict:
 def case_of(d: dict) -> Case:
     p = d["params"]
     return Case(tuple(p["shape"]), p["tau"], p["collision"], tuple(p["periodic"]), p["u_lid"],
-                tuple(p["force"]), p["magic"], p["s_e"], p["s_eps"], d.get("solid"))
+                tuple(p["force"]), p["magic"], p["s_e"], p["s_eps"], d.get("solid"),
+                inlet=d.get("inlet"), outlet=bool(d.get("outlet", False)))
 
 
 def rest_state(case: Case) -> np.ndarray:

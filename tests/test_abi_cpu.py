@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
     assert "lbm_launch" in names and "lbm_advance" in names
     for n in names:
         assert hasattr(lib, n), n
-    assert lib.lbm_abi_version() == 1
+    assert lib.lbm_abi_version() == 2
 
 
 @pytest.mark.parametrize("lat,ref", [(_lib.D2Q9, O.D2Q9), (_lib.D3Q19, O.D3Q19)])
@@ -95,6 +95,44 @@ def test_launch_rejects_bad_buffers_without_touching_the_gpu():
     assert lib.lbm_advance(ctypes.byref(d), 64, 128, 0, -1, 0) == -12
     d.solid_bits = 64
     assert lib.lbm_launch(ctypes.byref(d), 64, 64, 1, 0) == -15     # AA with solids
+
+
+def test_inlet_outlet_validation_without_touching_the_gpu():
+    """Inlet / outlet (pylbm's Problem.inlet / outlet) need D2Q9, walls on x and the AB pull."""
+    from pylbm_b200.backend import make_desc
+    from pylbm_b200.problem import Problem
+
+    lib = _lib.load()
+    d = make_desc(Problem((64, 32)), _lib.STORE_F32)
+    d.outlet = 1
+    assert lib.lbm_validate(ctypes.byref(d)) == 0
+    d.inlet_u = 256
+    assert lib.lbm_validate(ctypes.byref(d)) == 0
+    assert lib.lbm_launch(ctypes.byref(d), 64, 64, 1, 0) == -17     # AA with open boundaries
+    d.inlet_u = 258
+    assert lib.lbm_validate(ctypes.byref(d)) == -10                 # misaligned profile
+    d.inlet_u = 256
+    d.outlet = 2
+    assert lib.lbm_validate(ctypes.byref(d)) == -15
+    d.outlet = 1
+    d.periodic_mask = 1                                             # periodic x
+    assert lib.lbm_validate(ctypes.byref(d)) == -17
+    d3 = make_desc(Problem((16, 8, 8)), _lib.STORE_F32)
+    d3.outlet = 1
+    assert lib.lbm_validate(ctypes.byref(d3)) == -17
+    assert "inlet" in lib.lbm_error_string(-17).decode()
+
+
+def test_backend_supports_inlet_outlet_on_two_buffer_d2q9():
+    import numpy as np
+
+    from pylbm_b200 import backend as B
+    from pylbm_b200.problem import Problem
+
+    p = Problem((40, 12), inlet=np.full(12, 0.05), outlet=True)
+    assert B.B200Fused.supports(p)[0] and B.B200FusedFP16.supports(p)[0]
+    assert not B.VARIANTS["fused-aa"].supports(p)[0]
+    assert not B.B200Fused.supports(Problem((40, 12), periodic=(True, False), outlet=True))[0]
 
 
 def test_solid_bit_packing():

@@ -41,6 +41,25 @@ def test_oracle_solids_and_momentum_exchange(name):
     np.testing.assert_allclose(np.array(hist), d["force_hist"], rtol=1e-13, atol=1e-18)
 
 
+@pytest.mark.parametrize("name", names("inout_"))
+def test_oracle_inlet_outlet(name):
+    """Velocity inlet and pressure outlet (core.py:67-78,116-117,130-148) reproduce pylbm bit
+    for bit, with a solid disc and the momentum-exchange force where the fixture has them."""
+    d = load(name)
+    case = case_of(d)
+    f = initial(d, case)
+    masks = O.force_masks(case) if case.solid is not None else None
+    src = O.solid_sources(case) if case.solid is not None else None
+    hist = []
+    for _ in range(int(d["steps"])):
+        f = O.step(f, case, np, src)
+        if masks is not None:
+            hist.append(O.momentum_exchange(f, case, masks))
+    assert np.array_equal(f, d["f"])
+    if "force_hist" in d:
+        np.testing.assert_allclose(np.array(hist), d["force_hist"], rtol=1e-13, atol=1e-18)
+
+
 @pytest.mark.parametrize("name", names("tags_"))
 def test_oracle_stream_index_map(name):
     d = load(name)
