@@ -219,12 +219,49 @@ class B200Fused:
         self._advance(n)
         self.steps_done += n
 
+    # Lattices below GRAPH_MAX_NODES are launch-bound (a 128^2 step moves ~2.4 us of data,
+    # less than a host launch costs): their steps replay from a CUDA graph of GRAPH_CHUNK
+    # launches, captured once per descriptor and buffer orientation.
+    use_graphs: ClassVar[bool] = True
+    GRAPH_MAX_NODES: ClassVar[int] = 1 << 20
+    GRAPH_CHUNK: ClassVar[int] = 64  # even: A and B end where they started
+
     def _advance(self, n: int) -> None:
+        if self.use_graphs and self.N < self.GRAPH_MAX_NODES and n >= self.GRAPH_CHUNK:
+            g = self._graph()
+            for _ in range(n // self.GRAPH_CHUNK):
+                g.replay()
+            n %= self.GRAPH_CHUNK
+        if n == 0:
+            return
         b = self.A if self.aa else self.B
         _lib.call("lbm_advance", ctypes.byref(self.desc), self.A.data_ptr(), b.data_ptr(),
                   int(self.aa), int(n), _stream())
         if not self.aa and n % 2:
             self.A, self.B = self.B, self.A
+
+    def _graph(self) -> Any:
+        key = (bytes(self.desc), self.A.data_ptr())
+        graphs = self.__dict__.setdefault("_graphs", {})
+        g = graphs.get(key)
+        if g is not None:
+            return g
+        # one-time kernel set-up (attributes, occupancy queries) outside the capture, on copies
+        sa = self.A.clone()
+        sb = sa if self.aa else torch.empty_like(sa)
+        _lib.call("lbm_advance", ctypes.byref(self.desc), sa.data_ptr(), sb.data_ptr(),
+                  int(self.aa), 2, _stream())
+        torch.cuda.current_stream().synchronize()
+        del sa, sb
+        g = torch.cuda.CUDAGraph()
+        b = self.A if self.aa else self.B
+        with torch.cuda.graph(g):
+            _lib.call("lbm_advance", ctypes.byref(self.desc), self.A.data_ptr(), b.data_ptr(),
+                      int(self.aa), self.GRAPH_CHUNK, _stream())
+        if len(graphs) >= 4:
+            graphs.clear()
+        graphs[key] = g
+        return g
 
     def launch(self, pattern: int) -> None:
         """One kernel launch of the given pattern (pylbm's FusedSolver._launch)."""
