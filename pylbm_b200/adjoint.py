@@ -116,14 +116,26 @@ class DragAdjoint:
         self.solver.step(n)
 
     def reverse_step(self, n: int = 1) -> None:
-        """n recompute + adjoint step pairs on scratch buffers (timing only)."""
+        """n recompute + adjoint step pairs on scratch buffers (timing only). Pairs replay
+        from a CUDA graph of 32, as the forward steps of a launch-bound lattice do, so the two
+        are timed alike."""
         s, N = self.solver, self.N
-        desc = ctypes.byref(s.desc)
         if not hasattr(self, "_scratch"):
             self._scratch = (torch.zeros(9 * N, device=self.dev), torch.zeros(9 * N, device=self.dev),
                              torch.zeros(3 * N, device=self.dev),
                              torch.zeros(2 * N, dtype=torch.float64, device=self.dev),
                              torch.empty_like(s.A), s.A.clone())
+            self._pairs(2)  # kernel set-up outside any capture
+            self._rev_graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self._rev_graph):
+                self._pairs(32)
+        for _ in range(n // 32):
+            self._rev_graph.replay()
+        self._pairs(n % 32)
+
+    def _pairs(self, n: int) -> None:
+        """n (even) recompute + adjoint step pairs on the scratch buffers, in place."""
+        desc = ctypes.byref(self.solver.desc)
         mi, mo, ru, g, b, a = self._scratch
         for _ in range(n):
             _lib.call("lbm_forward_record", desc, a.data_ptr(), b.data_ptr(), ru.data_ptr(),
@@ -132,7 +144,8 @@ class DragAdjoint:
             _lib.call("lbm_adjoint_step", desc, ru.data_ptr(), mi.data_ptr(), mo.data_ptr(),
                       g.data_ptr(), 1.0, _stream())
             mi, mo = mo, mi
-        self._scratch = (mi, mo, ru, g, b, a)
+        if n % 2:  # keep the buffer roles of an even count for the captured graph
+            self._scratch = (mi, mo, ru, g, b, a)
 
 
 class _DragObjective(torch.autograd.Function if torch is not None else object):
