@@ -320,6 +320,7 @@ def config_of(name: str, a: argparse.Namespace) -> dict:
                 "variant": variant, "edges": "log-uniform [128, 1024], multiples of 8",
                 "tau": "U[0.51, 1.0]", "u_lid": "U[0.05, 0.1]", "seed": seed,
                 "lbm_steps_per_step": a.lbm_steps, "launch": "CUDA graph, one launch per step",
+                "launch_shape": getattr(a, "launch_shape", None),
                 "init": "lid-driven cavities, fluid at rest",
                 "l2": "state larger than L2 (no flush needed)",
                 "parallelism": f"replicas x{a.gpus}"}
@@ -359,7 +360,7 @@ def run_b200(a: argparse.Namespace) -> None:
         from pylbm_b200.batched import BatchedSolver
 
         s = BatchedSolver(batch_problems(name), BATCHES[name][2])
-        autotune_batch(s)
+        a.launch_shape = autotune_batch(s)["launch"]  # threads per block, blocks per SM (0: one item per warp)
         nodes = s.nodes
     else:
         cls = VARIANTS[WORKLOADS[name][4]]
