@@ -339,6 +339,39 @@ def config_of(name: str, a: argparse.Namespace) -> dict:
             "l2": "state larger than L2 (no flush needed)", "parallelism": f"replicas x{a.gpus}"}
 
 
+# ----------------------------------------------------------------------------- ranks
+def rank_barrier(world: int, device: str) -> None:
+    """All ranks meet here, with the device idle on both sides (no-op for one rank)."""
+    import torch
+
+    if device == "cuda":
+        torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        if device == "cuda":
+            torch.cuda.synchronize()
+
+
+def ranks_max(v: float, world: int, device: str) -> float:
+    """The maximum of v over the ranks (the job's time is its slowest rank's)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_mlups(world: int, nodes: int, steps: int, seconds: float) -> float:
+    """Whole-job throughput of ``world`` replicas, each advancing ``nodes`` nodes ``steps``
+    times, over the max-over-ranks time."""
+    return world * nodes * steps / seconds / 1e6
+
+
 # ----------------------------------------------------------------------------- GPU arm
 def run_b200(a: argparse.Namespace) -> None:
     import torch
@@ -371,17 +404,10 @@ def run_b200(a: argparse.Namespace) -> None:
     L = a.lbm_steps
 
     def barrier() -> None:
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-            torch.cuda.synchronize()
+        rank_barrier(world, "cuda")
 
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks_max(v, world, "cuda")
 
     # ---------------- device-resident throughput
     for _ in range(a.warmup):
@@ -398,7 +424,7 @@ def run_b200(a: argparse.Namespace) -> None:
     dt = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     clocks = clk.summary()
     launches = a.steps * L  # one kernel launch per lattice time step (AB and AA alike)
-    value = world * nodes * L * a.steps / dt / 1e6
+    value = replica_mlups(world, nodes, L * a.steps, dt)
 
     # ---------------- end to end through the solver API, host buffers
     e2e = None
@@ -422,7 +448,7 @@ def run_b200(a: argparse.Namespace) -> None:
         barrier()
         dte = max_over_ranks(e0.elapsed_time(e1) / 1e3)
         nbytes = s.A.numel() * s.A.element_size()
-        e2e = {"value": world * nodes * L * a.steps / dte / 1e6, "unit": "MLUPS",
+        e2e = {"value": replica_mlups(world, nodes, L * a.steps, dte), "unit": "MLUPS",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
 
     if rank == 0:
