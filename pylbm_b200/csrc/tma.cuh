@@ -1,7 +1,7 @@
 // Bulk asynchronous copies (TMA, cp.async.bulk) and mbarriers in inline PTX, sm_90+ / sm_100a.
 //
 // Only the plain one-CTA forms are used: global -> shared copies completing on an mbarrier
-// with a byte count, never the .multicast::cluster form. Every wait is bounded by the global
+// with a byte count, never a form that multicasts to a cluster. Every wait is bounded by the global
 // nanosecond timer; a wait that gives up returns false and the caller records an error code
 // in device memory instead of spinning on.
 #pragma once
