@@ -71,6 +71,15 @@ BATCHES = {
 }
 
 
+# pylbm's published MLUPS for the same lattice, collision, size, storage and pattern on its
+# benchmark problem (the 4096^2 lid-driven cavity, README.md:84-115, on an RTX 3070 Laptop
+# GPU; its Re = 1000 sets a different relaxation rate, which changes no work per node);
+# vs_baseline is null for workloads without such a figure
+PUBLISHED_MLUPS = {
+    "d2q9-bgk-cavity-f32": 5024.0,  # CUDA C fused, fp32 (README.md:97)
+}
+
+
 def is_cavity(name: str) -> bool:
     return "cavity" in name
 
@@ -460,7 +469,8 @@ def run_b200(a: argparse.Namespace) -> None:
         out = {
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": (value / PUBLISHED_MLUPS[name]) if name in PUBLISHED_MLUPS else None,
             "dtype": "f32" if s.storage == "f32" else s.storage, "data": "synthetic",
             "config": config_of(name, a),
             "bytes_per_update": bpn, "effective_GBs": value * 1e6 * bpn / 1e9,
