@@ -136,9 +136,10 @@ int lbm_moments_f64(const LbmDesc* d, const void* f, int layout, double* out,
  * memory (an application whose own pool owns all of it, or a loop that must not risk an
  * allocation stall or failure mid-run). No counterpart in pylbm. The partial sums live in a
  * fixed 75,776-byte array in the library's device image (2368 rows; larger needs are refused
- * with LBM_E_SIZE), one copy per device until exit. The first call on a device looks up that
- * array's address and should come before any stream capture. All calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * with LBM_E_SIZE), one copy per device until exit. The first call on a device (and the first
+ * in a new context of it, e.g. after a device reset) looks up that array's address and should
+ * come before any stream capture. All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 int lbm_moments_f64_noalloc(const LbmDesc* d, const void* f, int layout, double* out,
                             uint64_t stream);
 

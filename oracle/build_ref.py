@@ -5,26 +5,27 @@
 For each configuration below this writes a header of #defines (the role of pylbm's
 kernel_source(), cupy_backend.py:51-70, generated here from this repository's lattice tables)
 into ``oracle/_ref/`` and compiles ``oracle/ref_launch.cu`` -- which #includes pylbm's
-``backends/cuda/lbm.cu`` from the reference tree, unmodified and uncopied -- into
-``oracle/_ref/lbmref_<name>.so`` for sm_100a. Nothing is built when the reference tree is
-absent (the GPU box uses the prebuilt files, which travel with the repository but are not
-committed).
+``backends/cuda/lbm.cu`` where pylbm is installed (``PYLBM_SRC`` or ``baseline/_ref``),
+unmodified and uncopied -- into ``oracle/_ref/lbmref_<name>.so`` for sm_100a. Nothing is built
+when pylbm is absent (the GPU box uses the prebuilt files, which travel with the working tree
+but are not committed).
 """
 
 from __future__ import annotations
 
-import os
 import subprocess
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF_SRC = Path(os.environ.get("PYLBM_SRC", "/root/reference/src"))
-REF_CU = REF_SRC / "pylbm" / "backends" / "cuda" / "lbm.cu"
-
 sys.path.insert(0, str(HERE.parent))
+from baseline import pylbm_path  # noqa: E402
 from oracle.lbm_oracle import D2Q9, D3Q19, MRT_M, MRT_NORM  # noqa: E402
+
+# pylbm's kernel source, from PYLBM_SRC or the offline install baseline/_ref
+_PYLBM = pylbm_path()
+REF_CU = (_PYLBM / "pylbm" / "backends" / "cuda" / "lbm.cu") if _PYLBM else Path("/nonexistent")
 
 # name: (lattice, periodic, lid, force, collision, storage, pattern)
 CONFIGS = {

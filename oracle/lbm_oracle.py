@@ -196,7 +196,7 @@ def stream(f: Any, case: Case, xp: Any = np, solid_src: list | None = None) -> l
         out.append(X.roll(f[i], shifts, axes) if any(shifts) else X.copy(f[i]))
     if case.solid is not None:
         src = solid_src if solid_src is not None else solid_sources(
-            case, (lambda a: xp.as_tensor(a)) if X.torch else np.asarray)
+            case, (lambda a: xp.as_tensor(a, device=f.device)) if X.torch else np.asarray)
         opp = lat.opp
         for i in range(lat.q):
             if any(lat.c[i]):
@@ -228,7 +228,7 @@ def stream(f: Any, case: Case, xp: Any = np, solid_src: list | None = None) -> l
 def _as(a: Any, like: Any, X: Any) -> Any:
     """``a`` as an array of the backend of ``like`` (numpy or torch)."""
     if X.torch:
-        return X.xp.as_tensor(np.asarray(a), dtype=like.dtype)
+        return X.xp.as_tensor(np.asarray(a), dtype=like.dtype, device=like.device)
     return np.asarray(a, dtype=np.float64)
 
 
@@ -372,8 +372,8 @@ def step(f: Any, case: Case, xp: Any = np, solid_src: list | None = None) -> Any
 
 def run(case: Case, f0: Any, steps: int, xp: Any = np) -> Any:
     f = f0
-    src = solid_sources(case, (lambda a: xp.as_tensor(a)) if xp.__name__ == "torch"
-                        else np.asarray)
+    src = solid_sources(case, (lambda a: xp.as_tensor(a, device=f0.device))
+                        if xp.__name__ == "torch" else np.asarray)
     for _ in range(steps):
         f = step(f, case, xp, src)
     return f
@@ -416,8 +416,8 @@ def momentum_exchange(f: Any, case: Case, masks: list | None = None, xp: Any = n
     lat = case.lat
     masks = masks if masks is not None else force_masks(case)
     if xp.__name__ == "torch":
-        mk = xp.stack([xp.as_tensor(m, dtype=f.dtype) for m in masks])
-        ct = xp.as_tensor(np.array(lat.c, dtype=np.float64), dtype=f.dtype)
+        mk = xp.stack([xp.as_tensor(m, dtype=f.dtype, device=f.device) for m in masks])
+        ct = xp.as_tensor(np.array(lat.c, dtype=np.float64), dtype=f.dtype, device=f.device)
         per_dir = (f * mk).reshape(lat.q, -1).sum(dim=1)
         return 2.0 * (per_dir[:, None] * ct).sum(0)
     mk = np.stack(masks).astype(np.float64)
@@ -430,8 +430,8 @@ def drag_objective(case: Case, f0: Any, steps: int, t0: int, xp: Any = np,
     """J = mean over t = t0..steps of the x momentum-exchange force on the state after t
     steps. With torch and ``checkpoint`` > 0 the forward is segment-checkpointed."""
     masks = force_masks(case)
-    src = solid_sources(case, (lambda a: xp.as_tensor(a)) if xp.__name__ == "torch"
-                        else np.asarray)
+    src = solid_sources(case, (lambda a: xp.as_tensor(a, device=f0.device))
+                        if xp.__name__ == "torch" else np.asarray)
     f = f0
     acc: Any = 0.0
     count = 0

@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import ctypes
 import sys
+import types
 from typing import Any, ClassVar
 
 import numpy as np
@@ -186,12 +187,19 @@ class B200Fused:
     def layout(self) -> int:
         return _lib.LAYOUT_AA_SWAPPED if self.aa else _lib.LAYOUT_NATURAL
 
-    def set_populations(self, f: np.ndarray) -> None:
-        """Load a canonical float64 post-collision state (q, *array_shape)."""
-        f = np.asarray(f, dtype=np.float64)
-        if f.shape != (self.q,) + tuple(self.problem.array_shape):
-            raise ValueError(f"populations must have shape {(self.q,) + tuple(self.problem.array_shape)}")
-        t = torch.from_numpy(np.ascontiguousarray(f)).to(self.dev)
+    def set_populations(self, f: Any) -> None:
+        """Load a canonical float64 post-collision state (q, *array_shape): a numpy array, or
+        a torch tensor (already on the device: no host copy)."""
+        want = (self.q,) + tuple(self.problem.array_shape)
+        if torch.is_tensor(f):
+            t = f.to(device=self.dev, dtype=torch.float64).contiguous()
+        else:
+            f = np.asarray(f, dtype=np.float64)
+            t = None
+        if tuple(f.shape) != want:
+            raise ValueError(f"populations must have shape {want}, got {tuple(f.shape)}")
+        if t is None:
+            t = torch.from_numpy(np.ascontiguousarray(f)).to(self.dev)
         _lib.call("lbm_encode_f64", ctypes.byref(self.desc), t.data_ptr(), self.A.data_ptr(),
                   self.layout, _stream())
         torch.cuda.current_stream().synchronize()
@@ -396,19 +404,41 @@ VARIANTS: dict[str, type] = {c.variant: c for c in (
     B200FusedPlain)}
 
 
+def pylbm_classes(solver_base: Any) -> dict[str, type]:
+    """The variants as subclasses of pylbm's abstract ``Solver`` (backends/base.py:18-96):
+    isinstance checks against pylbm's base hold, and ``step`` / ``macroscopic`` are pylbm's
+    own (base.py:68-82) rather than this module's equivalents, so the two cannot drift."""
+    out = {}
+    for v, cls in VARIANTS.items():
+        ns = {"__module__": "pylbm.backends.b200_backend", "__doc__": cls.__doc__,
+              "step": solver_base.step, "macroscopic": solver_base.macroscopic}
+        out[v] = types.new_class(cls.__name__, (cls, solver_base),
+                                 exec_body=lambda d, ns=ns: d.update(ns))
+    return out
+
+
 def register(backends: Any = None) -> list[tuple[str, str]]:
     """Add the ``b200`` variants to pylbm's backend registry (backends/__init__.py:16-34).
 
     pylbm resolves an entry by importing ``pylbm.backends.<module>`` lazily
-    (backends/__init__.py:53-63); this module is installed under that name in ``sys.modules``
-    so the lookup finds it without touching pylbm's files."""
+    (backends/__init__.py:53-63); a module of that name holding the :func:`pylbm_classes` is
+    installed in ``sys.modules``, so the lookup finds it without touching pylbm's files."""
     if backends is None:
         import pylbm.backends as backends  # type: ignore[import-not-found,no-redef]
-    sys.modules[f"{backends.__name__}.b200_backend"] = sys.modules[__name__]
+    global Unsupported
+    if not issubclass(Unsupported, backends.Unsupported):
+        # this module was imported before pylbm was importable: from now on raise a class
+        # that pylbm's callers catch as theirs and stand-alone callers as this module's
+        Unsupported = type("Unsupported", (backends.Unsupported, Unsupported),
+                           {"__module__": __name__, "__doc__": Unsupported.__doc__})
+    mod = types.ModuleType(f"{backends.__name__}.b200_backend",
+                           "pylbm backend b200: pylbm_b200's fused solvers as pylbm Solvers")
     added = []
-    for v, cls in VARIANTS.items():
+    for v, cls in pylbm_classes(backends.Solver).items():
+        setattr(mod, cls.__name__, cls)
         backends._ENTRIES[("b200", v)] = f"b200_backend:{cls.__name__}"
         added.append(("b200", v))
+    sys.modules[mod.__name__] = mod
     if hasattr(backends, "COLORS"):
         backends.COLORS.setdefault("b200", "#76b900")
     return added

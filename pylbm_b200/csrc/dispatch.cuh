@@ -77,8 +77,12 @@ int launch_decode(const LbmDesc& d, const void* buf, int layout, double* f64, cu
 int launch_macroscopic(const LbmDesc& d, const void* f, int layout, float* rho, float* u,
                        cudaStream_t s);
 int launch_moments(const LbmDesc& d, const void* f, int layout, double* out, cudaStream_t s);
-// Rows of partial sums the moment reduction uses for N nodes, and the reduction into
-// caller-provided scratch of 4 * rows doubles.
+// Grid cap of the node-parallel helper kernels (encode, decode, macroscopic, the moment
+// reduction's first pass): 16 blocks per SM of the 148. It is also the most rows of partial
+// sums the moment reduction ever uses, which bounds the allocation-free entry point's array.
+constexpr int kHelperGridMax = 148 * 16;
+// Rows of partial sums the moment reduction uses for N nodes (at most kHelperGridMax), and
+// the reduction into caller-provided scratch of 4 * rows doubles.
 int moments_rows(int N);
 int launch_moments_into(const LbmDesc& d, const void* f, int layout, double* out,
                         double* scratch, int rows, cudaStream_t s);

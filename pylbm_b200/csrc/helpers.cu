@@ -140,7 +140,7 @@ k_moments_final(const double* __restrict__ partial, int rows, int N, double* out
 
 int grid_for(long long work) {
     long long g = (work + kThreads - 1) / kThreads;
-    if (g > 148 * 16) g = 148 * 16;
+    if (g > kHelperGridMax) g = kHelperGridMax;
     return int(g < 1 ? 1 : g);
 }
 

@@ -108,3 +108,42 @@ def cylinder_channel(nx: int = 1024, ny: int = 256, xc: float = 200.0, yc: float
     rng = np.random.default_rng(seed)
     field = sigma * rng.standard_normal((2, ny, nx))
     return solid, field
+
+
+# ----------------------------------------------------------------------------- on the device
+def equilibrium_device(lat, rho, u):  # noqa: ANN001, ANN201
+    """:func:`pylbm_b200.lattice.equilibrium` on float64 torch tensors, same operation order
+    (for multi-GB initial states, built where they are used)."""
+    import torch
+
+    usq = sum(u[a] ** 2 for a in range(lat.d))
+    out = torch.empty((lat.q,) + tuple(rho.shape), dtype=torch.float64, device=rho.device)
+    for i in range(lat.q):
+        cu = sum(int(lat.c[i, a]) * u[a] for a in range(lat.d))
+        out[i] = float(lat.w[i]) * rho * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq)
+    return out
+
+
+def fourier_populations_device(n: int, seed: int = 0, device: str = "cuda"):  # noqa: ANN201
+    """:func:`fourier_populations` as a float64 device tensor (fields from the same seeded
+    host generator, equilibrium on the device)."""
+    import torch
+
+    rho, u = fourier_state(n, seed)
+    return equilibrium_device(D2Q9, torch.as_tensor(rho, device=device),
+                              torch.as_tensor(u, device=device))
+
+
+def taylor_green_3d_populations_device(n: int, u0: float = 0.05,
+                                       device: str = "cuda"):  # noqa: ANN201
+    """:func:`taylor_green_3d_populations` built on the device (float64 tensor)."""
+    import torch
+
+    k = 2.0 * np.pi / n
+    s = torch.sin(k * torch.arange(n, dtype=torch.float64, device=device))
+    c = torch.cos(k * torch.arange(n, dtype=torch.float64, device=device))
+    # array axes (z, y, x)
+    ux = u0 * c[:, None, None] * c[None, :, None] * s[None, None, :]
+    uy = -u0 * c[:, None, None] * s[None, :, None] * c[None, None, :]
+    u = torch.stack([ux, uy, torch.zeros_like(ux)])
+    return equilibrium_device(D3Q19, torch.ones((n, n, n), dtype=torch.float64, device=device), u)

@@ -1,11 +1,10 @@
 """Generate the golden fixtures in this folder by running pylbm itself.
 
-    PYLBM_SRC=/path/to/pylbm/src python tests/golden/make_golden.py
+    [PYLBM_SRC=/path/to/pylbm/src] python tests/golden/make_golden.py
 
-pylbm (the reference implementation) is imported read-only from ``PYLBM_SRC`` (default: the
-reference checkout this repository was built against, ``/root/reference/src``). It is needed
-only to (re)generate the fixtures; the tests read the committed ``.npz`` files and never import
-pylbm. Every fixture stores the problem parameters (JSON), the initial state when it is not
+pylbm (the reference implementation) is imported read-only from ``PYLBM_SRC`` or, without it,
+from the offline install ``baseline/_ref`` (``baseline/install_ref.py``). It is needed only to
+(re)generate the fixtures; the parity tests read the committed ``.npz`` files. Every fixture stores the problem parameters (JSON), the initial state when it is not
 the rest equilibrium, the step count and pylbm's float64 NumPy result:
 
 * ``eq_*``      pylbm's own equivalence cases (tests/test_equivalence.py:9-20), 100 steps,
@@ -27,16 +26,17 @@ from __future__ import annotations
 
 import dataclasses
 import json
-import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-SRC = os.environ.get("PYLBM_SRC", "/root/reference/src")
 sys.dont_write_bytecode = True
-sys.path.insert(0, SRC)
+sys.path.insert(0, str(HERE.parents[1]))
+from baseline import import_pylbm  # noqa: E402
+
+import_pylbm()  # PYLBM_SRC or the offline install baseline/_ref
 
 from pylbm import core  # noqa: E402
 from pylbm.backends.numpy_backend import NumpySolver  # noqa: E402

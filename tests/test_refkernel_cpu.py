@@ -1,17 +1,16 @@
 """The #define headers used to build pylbm's own kernel as a comparator equal the header that
-pylbm's kernel_source() (cupy_backend.py:51-70) prints for the same problem. Needs the
-reference tree (skipped elsewhere); the GPU box only uses the prebuilt comparators."""
+pylbm's kernel_source() (cupy_backend.py:51-70) prints for the same problem. Needs pylbm
+(``baseline/_ref`` or ``PYLBM_SRC``; skipped without it)."""
 
 from __future__ import annotations
 
 import re
-import sys
 
 import pytest
 
 from oracle import build_ref
 
-pytestmark = pytest.mark.skipif(not build_ref.REF_CU.exists(), reason="reference tree absent")
+pytestmark = pytest.mark.skipif(not build_ref.REF_CU.exists(), reason="pylbm not installed")
 
 
 def _defines(text: str) -> dict:
@@ -26,7 +25,9 @@ def _defines(text: str) -> dict:
 
 @pytest.mark.parametrize("name", list(build_ref.CONFIGS))
 def test_header_matches_pylbm_kernel_source(name):
-    sys.path.insert(0, str(build_ref.REF_SRC))
+    from baseline import import_pylbm
+
+    import_pylbm()
     from pylbm.backends.cupy_backend import kernel_source
     from pylbm.problem import Problem
 
