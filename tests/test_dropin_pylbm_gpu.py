@@ -16,8 +16,6 @@ pylbm itself is imported read-only from its offline install (``baseline/_ref``) 
 
 from __future__ import annotations
 
-import json
-
 import numpy as np
 import pytest
 
@@ -48,7 +46,7 @@ def pylbm():
 def pylbm_problem(pylbm, name: str):  # noqa: ANN001, ANN201
     from pylbm.problem import Problem
 
-    prm = json.loads(str(load(name)["params"]))
+    prm = load(name)["params"]
     return Problem(tuple(prm["shape"]), tau=prm["tau"], collision=prm["collision"],
                    periodic=tuple(prm["periodic"]), u_lid=prm["u_lid"],
                    force=tuple(prm["force"]), magic=prm["magic"], s_e=prm["s_e"],
@@ -95,8 +93,12 @@ def test_pylbm_equivalence_cases(pylbm, variant, case):
     assert np.abs(u - u_r).max() < 10 * TOL[s.storage]
 
 
-@pytest.mark.parametrize("storage", ["", "-fp16"])
-def test_aa_equals_ab_through_pylbm(pylbm, storage):
+@pytest.mark.parametrize("storage,tol", [("", 1e-6), ("-fp16", TOL["f16"])])
+def test_aa_equals_ab_through_pylbm(pylbm, storage, tol):
+    """pylbm's AA-vs-AB check (1e-6 for fp32). In 16-bit storage the two patterns round the
+    lid term at different places (AB adds it to the pulled, already rounded value; AA's odd
+    step stores p - t rounded and the next pull adds t back), so they agree to the storage
+    tolerance rather than bit for bit."""
     import pylbm.backends as B
     from pylbm.problem import Problem
 
@@ -104,7 +106,7 @@ def test_aa_equals_ab_through_pylbm(pylbm, storage):
     a, b = B.make("b200", "fused" + storage, p), B.make("b200", "fused-aa" + storage, p)
     a.step(60)
     b.step(60)
-    assert np.abs(a.populations() - b.populations()).max() < 1e-6
+    assert np.abs(a.populations() - b.populations()).max() < tol
 
 
 def test_make_solver_and_unsupported(pylbm):

@@ -7,8 +7,9 @@ sums: two calls in a row, on two different states, each compared with the alloca
 point within the moment tests' tolerance (rtol 1e-12) and with an independent float64 sum of
 the decoded state; in both buffer layouts. It must also allocate nothing: across its calls
 the high-water mark of the device's stream-ordered memory pool does not rise above what was
-already in use, while the allocating entry point, as a control, raises it. The file is collected last so that a run
-stopping at the first failure has already run every other test; it also passes alone.
+already in use, while the allocating entry point, as a control, raises it. The file is
+collected last so that a run stopping at the first failure has already run every other test;
+it also passes alone.
 """
 
 from __future__ import annotations
