@@ -168,3 +168,113 @@ def run_karman(d: int = 40, u_mean: float = 0.05, periods: float = 20.0,
             "shape": list(p.shape), "steps": s.steps_done, "St": float(st),
             "cd_max": float(cd.max()), "cl_max": float(cl.max()), "cd_mean": float(cd.mean()),
             "reference": KARMAN_REFERENCE, "vorticity": (vort * d / u_mean).cpu().numpy()}
+
+
+# ----------------------------------------------------------------------------- Ghia cavity
+# Table II, Re = 400, x = 0.9063 breaks the monotonic run of its neighbours and is a known
+# misprint of the 1982 tables; pylbm leaves it out of its error norms (validation/ghia.py:17)
+GHIA_SKIP = {("v", 400, 0.9063)}
+
+
+def ghia_data_path() -> Any:
+    """pylbm's tabulation of Ghia, Ghia & Shin (1982), read where pylbm is installed
+    (pylbm/validation/data/ghia1982.json); not copied into this package."""
+    import importlib.util
+    from pathlib import Path
+
+    spec = importlib.util.find_spec("pylbm")
+    if spec is None or spec.origin is None:
+        raise FileNotFoundError("the Ghia tables are read from an installed pylbm; none found")
+    return Path(spec.origin).parent / "validation" / "data" / "ghia1982.json"
+
+
+def ghia_reference(re: int, path: Any = None) -> dict:
+    """Centreline velocities of the 1982 tables for Re in {100, 400, 1000}: u(y) on x = 1/2
+    and v(x) on y = 1/2, in units of the lid speed and the cavity side."""
+    import json
+    from pathlib import Path
+
+    t = json.loads(Path(path or ghia_data_path()).read_text())
+    key = str(int(re))
+    return {"y": np.asarray(t["u_vertical"]["y"], float),
+            "u": np.asarray(t["u_vertical"][key], float),
+            "x": np.asarray(t["v_horizontal"]["x"], float),
+            "v": np.asarray(t["v_horizontal"][key], float)}
+
+
+def cavity_centrelines(ux: np.ndarray, uy: np.ndarray, u_lid: float) -> dict:
+    """u / U on the vertical and v / U on the horizontal centreline of (ny, nx) fields, at the
+    node centres (i + 1/2) / n of a half-way bounce-back cavity (the mean of the two middle
+    nodes for even n), with the wall values appended at 0 and 1 (u = U on the lid)."""
+    ny, nx = ux.shape
+
+    def centre(a: np.ndarray, axis: int) -> np.ndarray:
+        n = a.shape[axis]
+        lo, hi = (n - 1) // 2, n // 2
+        return 0.5 * (np.take(a, lo, axis=axis) + np.take(a, hi, axis=axis))
+
+    y = np.r_[0.0, (np.arange(ny) + 0.5) / ny, 1.0]
+    x = np.r_[0.0, (np.arange(nx) + 0.5) / nx, 1.0]
+    return {"y": y, "u": np.r_[0.0, centre(ux, 1) / u_lid, 1.0],
+            "x": x, "v": np.r_[0.0, centre(uy, 0) / u_lid, 0.0]}
+
+
+def ghia_errors(prof: dict, re: int, ref: dict) -> dict:
+    """RMS and maximum deviation from the tables at their interior points (linear
+    interpolation of the profiles), per component and combined; units of the lid speed."""
+    out = {}
+    for comp, axis in (("u", "y"), ("v", "x")):
+        pts = ref[axis]
+        keep = (pts > 0.0) & (pts < 1.0)
+        keep &= np.array([(comp, int(re), round(float(p), 4)) not in GHIA_SKIP for p in pts])
+        dev = np.interp(pts[keep], prof[axis], prof[comp]) - ref[comp][keep]
+        out[f"{comp}_L2"] = float(np.sqrt(np.mean(dev * dev)))
+        out[f"{comp}_Linf"] = float(np.abs(dev).max())
+    out["L2"] = float(np.sqrt(0.5 * (out["u_L2"] ** 2 + out["v_L2"] ** 2)))
+    out["Linf"] = max(out["u_Linf"], out["v_Linf"])
+    return out
+
+
+def run_ghia(re: int, n: int = 128, u_lid: float = 0.1, collision: str = "bgk",
+             variant: str = "fused", tol: float = 1e-5, max_steps: int = 1_000_000,
+             check_every: int | None = None, data_path: Any = None) -> dict:
+    """The lid-driven cavity at Reynolds number ``re`` run to a steady state on this backend
+    and compared with Ghia et al. (1982), as pylbm's validation/ghia.py:96-132 does: every
+    ``check_every`` steps (default max(1000, 4 n)) the RMS change of the velocity field over
+    the lid speed is compared with ``tol``; a non-finite field stops the run; 16-bit storages,
+    whose round-off floor lies above ``tol``, stop once the change has not improved for ten
+    checks and is within 50 tol ("plateau"). The velocity comes from the device (fp32
+    ``lbm_macroscopic``), so a check copies two fields, not the float64 state."""
+    import torch
+
+    ref = ghia_reference(re, data_path)
+    p = Problem.cavity(n, re=re, u_lid=u_lid, collision=collision)
+    s = _solver(p, variant)
+    every = check_every or max(1000, 4 * n)
+    every -= every % s.step_multiple
+    u_old = s.macroscopic_device()[1].double()
+    converged: Any = False
+    best, stale, change = float("inf"), 0, float("nan")
+    while s.steps_done < max_steps:
+        s.step(every)
+        u = s.macroscopic_device()[1].double()
+        if not bool(torch.isfinite(u).all()):
+            break
+        change = float(torch.sqrt(torch.mean((u - u_old) ** 2))) / u_lid
+        u_old = u
+        if change < tol:
+            converged = True
+            break
+        if change < 0.9 * best:
+            best, stale = change, 0
+        else:
+            stale += 1
+        if stale >= 10 and best < 50 * tol:
+            converged = "plateau"
+            break
+    uh = u_old.cpu().numpy()
+    prof = cavity_centrelines(uh[0], uh[1], u_lid)
+    return {"re": re, "n": n, "variant": variant, "collision": collision, "tau": p.tau,
+            "steps": s.steps_done, "converged": converged, "last_change": change,
+            "errors": ghia_errors(prof, re, ref),
+            "profile": {k: v.tolist() for k, v in prof.items()}}
