@@ -163,9 +163,11 @@ __device__ __forceinline__ void collide_pairs(S (&h)[L::Q], const float (&F)[3],
     const float gm = 1.0f - 0.5f * rm;
     const float kp = 0.5f * (1.0f - r0);
     const float km = 0.5f * (1.0f - rm);
-    {  // rest population: heq_0 = w_0 (drho + rho t), S_0 = -3 w_0 u.F
+    // ep / w = drho + rho t + 4.5 rho (c.u)^2 = base + 4.5 (c.rho u)(c.u)
+    const S base = fma_(rho, t, drho);
+    {  // rest population: heq_0 = w_0 base, S_0 = -3 w_0 u.F
         const float w0 = L::w(0);
-        S p = fma_(sc<S>(1.0f - r0), h[0], sc<S>(r0 * w0) * fma_(rho, t, drho));
+        S p = fma_(sc<S>(1.0f - r0), h[0], sc<S>(r0 * w0) * base);
         if constexpr (FORCE) p = fma_(sc<S>(gp * w0), uf3, p);
         h[0] = p;
     }
@@ -177,8 +179,10 @@ __device__ __forceinline__ void collide_pairs(S (&h)[L::Q], const float (&F)[3],
         const S cj = cdot<L>(i, ju);  // c.(rho u)
         // c.u: u_ax itself along an axis, else (c.j) / rho (a product, never a sum of them)
         const S cu = naxes<L>(i) == 1 ? u[first_axis<L>(i)] : cj * inv_rho;
-        const S x = fma_(rho, fma_(sc<S>(4.5f) * cu, cu, t), drho);  // ep / w
-        S A = fma_(sc<S>(kp), a[i], sc<S>(r0 * w) * x);
+        // s+ ep = s+ w base + 4.5 s+ w (c.rho u)(c.u); the first term is shared by the pairs
+        // of one weight
+        const S sep = fma_(sc<S>(4.5f * r0 * w) * cj, cu, sc<S>(r0 * w) * base);
+        S A = fma_(sc<S>(kp), a[i], sep);
         S B = fma_(sc<S>(km), d[i], sc<S>(rm * 3.0f * w) * cj);
         if constexpr (FORCE) {
             float cf = 0.0f;  // c.F (uniform)
