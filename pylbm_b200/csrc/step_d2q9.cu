@@ -380,10 +380,11 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 // warps stride over the items; otherwise one item per warp (no loop state to keep, which
 // leaves more registers to the collision).
 //
-// 16-bit MRT batches are capped at 80 registers (3 blocks of 256 threads per SM; 12 bytes of
-// spills): latency-bound at 96 registers and 20 warps per SM, they measured 152K instead of
-// 146K MLUPS on the 64-cavity workload at 24 warps. The packed BGK / TRT batches spill too
-// much under that cap.
+// 16-bit batches collide the two nodes of a word together (packed f32x2, F2). 16-bit MRT
+// batches are capped at 3 blocks of 256 threads per SM (80 registers): on the 64-cavity
+// workload the packed MRT collision under that cap measured 155K MLUPS (0.86 of copy
+// bandwidth) against 143-146K for the one-node form; 2 blocks per SM measured 139K, no cap
+// 106K.
 template <int STORE, int COLL, bool PERSIST>
 __global__ void __launch_bounds__(256, (VT<STORE>::V == 8 && COLL == LBM_MRT) ? 3 : 1)
 k_d2q9_batch_ab(const BatchLattice* __restrict__ item_tab, int items,
@@ -436,8 +437,9 @@ k_d2q9_batch_ab(const BatchLattice* __restrict__ item_tab, int items,
         l.last = l.active && (lane == 31 || l.x0 + V >= P.n[0] || vidx + 1 >= nvec);
         const long long base = __ldg(&bl.base);
         const bool edge = __any_sync(0xffffffffu, l.active && edge_row(P, l.y));
-        if (edge) ab_row<STORE, COLL, false, true>(P, A + base, B + base, l);
-        else ab_row<STORE, COLL, false, false>(P, A + base, B + base, l);
+        constexpr bool pack = VT<STORE>::V == 8;
+        if (edge) ab_row<STORE, COLL, false, true, pack>(P, A + base, B + base, l);
+        else ab_row<STORE, COLL, false, false, pack>(P, A + base, B + base, l);
     }
 }
 
