@@ -246,12 +246,9 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
         } else if (cx == 1) {
             const uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
             if (!l.active) continue;
-            if (!l.first) {
-                st_plain(plane + l.x0, shift_up<V>(v[i], up));
-            } else {
-#pragma unroll
-                for (int k = 0; k < V - 1; ++k) st1(plane + l.x0 + 1 + k, elem<V>(v[i], k));
-            }
+            const uint4 su = shift_up<V>(v[i], up);
+            if (!l.first) st_plain(plane + l.x0, su);
+            else st_tail<V>(plane + l.x0, su);  // slot x0 belongs to the previous warp
             if (l.last) {
                 E* dst = l.x0 + V < nx ? plane + l.x0 + V : (P.per[0] ? plane : bb + nx - 1);
                 st1(dst, elem<V>(v[i], V - 1));
@@ -259,12 +256,9 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
         } else {
             const uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
             if (!l.active) continue;
-            if (!l.last) {
-                st_plain(plane + l.x0, shift_down<V>(v[i], dn));
-            } else {
-#pragma unroll
-                for (int k = 1; k < V; ++k) st1(plane + l.x0 + k - 1, elem<V>(v[i], k));
-            }
+            const uint4 sd = shift_down<V>(v[i], dn);
+            if (!l.last) st_plain(plane + l.x0, sd);
+            else st_head<V>(plane + l.x0, sd);  // slot x0 + V - 1 belongs to the next warp
             if (l.first) {
                 E* dst = l.x0 > 0 ? plane + l.x0 - 1 : (P.per[0] ? plane + nx - 1 : bb);
                 st1(dst, elem<V>(v[i], 0));

@@ -146,7 +146,14 @@ k_staged(const StepParams P, const StagedCfg C, const typename VT<STORE>::E* A,
             if (lane == 0) ok = mbar_wait(empty + s, ph ^ 1u, C.timeout_ns);
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) {
-                if (lane == 0) atomicOr(C.err, kDevErrTimeout);
+                if (lane == 0) {
+                    atomicOr(C.err, kDevErrTimeout);
+                    // let the copies this warp issued for the other slots land before the
+                    // block can exit (each wait bounded again; the error is already set)
+                    for (int k = it - C.stages + 1; k < it; ++k)
+                        if (k >= 0)
+                            mbar_wait(full + k % C.stages, (k / C.stages) & 1, C.timeout_ns);
+                }
                 return;
             }
             fence_proxy_async();

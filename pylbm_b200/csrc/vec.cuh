@@ -137,6 +137,32 @@ __device__ __forceinline__ void st_plain(void* p, const uint4& v) {
     *reinterpret_cast<uint4*>(p) = v;
 }
 
+// The elements 1..V-1 of vector u into p[1..V-1] (st_tail), or the elements 0..V-2 of d into
+// p[0..V-2] (st_head), p 16-byte aligned: the other slot belongs to a node of another warp.
+// Three aligned stores (16-bit: 2 + 4 + 8 bytes; fp32: 4 + 8) instead of V - 1 single ones.
+template <int V, class E>
+__device__ __forceinline__ void st_tail(E* p, const uint4& u) {
+    if constexpr (V == 8) {
+        *reinterpret_cast<uint16_t*>(p + 1) = static_cast<uint16_t>(u.x >> 16);
+        *reinterpret_cast<uint32_t*>(p + 2) = u.y;
+        *reinterpret_cast<uint2*>(p + 4) = make_uint2(u.z, u.w);
+    } else {
+        *reinterpret_cast<uint32_t*>(p + 1) = u.y;
+        *reinterpret_cast<uint2*>(p + 2) = make_uint2(u.z, u.w);
+    }
+}
+template <int V, class E>
+__device__ __forceinline__ void st_head(E* p, const uint4& d) {
+    if constexpr (V == 8) {
+        *reinterpret_cast<uint2*>(p) = make_uint2(d.x, d.y);
+        *reinterpret_cast<uint32_t*>(p + 4) = d.z;
+        *reinterpret_cast<uint16_t*>(p + 6) = static_cast<uint16_t>(d.w & 0xffffu);
+    } else {
+        *reinterpret_cast<uint2*>(p) = make_uint2(d.x, d.y);
+        *reinterpret_cast<uint32_t*>(p + 2) = d.z;
+    }
+}
+
 // Single elements.
 template <class E>
 __device__ __forceinline__ uint32_t ld1_nc(const E* p) {
