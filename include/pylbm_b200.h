@@ -35,7 +35,7 @@ extern "C" {
 /* collision operators */
 #define LBM_BGK 0
 #define LBM_TRT 1
-#define LBM_MRT 2 /* D2Q9 only */
+#define LBM_MRT 2 /* D2Q9: Lallemand-Luo basis (pylbm); D3Q19: d'Humieres et al. (2002) basis */
 #define LBM_STREAM_ONLY 3 /* debug: streaming and boundaries only, no collision */
 /* storage formats; arithmetic is fp32 in every case */
 #define LBM_STORE_F32 0         /* f in fp32, unshifted arithmetic (pylbm's own fp32 scheme) */
@@ -54,7 +54,7 @@ extern "C" {
 #define LBM_OK 0
 #define LBM_E_NULL -1        /* a required pointer is NULL */
 #define LBM_E_LATTICE -2     /* unknown lattice id */
-#define LBM_E_COLLISION -3   /* unknown collision, or MRT on D3Q19 */
+#define LBM_E_COLLISION -3   /* unknown collision operator */
 #define LBM_E_STORAGE -4     /* unknown storage id */
 #define LBM_E_PATTERN -5     /* unknown pattern id */
 #define LBM_E_SHAPE -6       /* a dimension < 1, or nz != 1 for D2Q9 */

@@ -71,6 +71,28 @@ MRT_M = ((1, 1, 1, 1, 1, 1, 1, 1, 1),
 MRT_NORM = tuple(float(sum(v * v for v in row)) for row in MRT_M)
 
 
+def _d3q19_mrt_rows() -> tuple:
+    """Orthogonal D3Q19 moment basis of d'Humieres et al. (2002, Phil. Trans. R. Soc. A 360,
+    437-451) as polynomials of c, evaluated on the D3Q19 velocities below: rows (rho, e, eps,
+    jx, qx, jy, qy, jz, qz, 3pxx, 3pixx, pww, piww, pxy, pyz, pxz, mx, my, mz). pylbm has no
+    D3Q19 MRT; this extends its D2Q9 form (core.py:228-246) to 3D."""
+    def rows(c: tuple) -> tuple:
+        x, y, z = c
+        c2 = x * x + y * y + z * z
+        return (1, 19 * c2 - 30, (21 * c2 * c2 - 53 * c2 + 24) // 2,
+                x, (5 * c2 - 9) * x, y, (5 * c2 - 9) * y, z, (5 * c2 - 9) * z,
+                3 * x * x - c2, (3 * c2 - 5) * (3 * x * x - c2),
+                y * y - z * z, (3 * c2 - 5) * (y * y - z * z),
+                x * y, y * z, x * z,
+                (y * y - z * z) * x, (z * z - x * x) * y, (x * x - y * y) * z)
+    cols = [rows(c) for c in D3Q19.c]
+    return tuple(tuple(col[k] for col in cols) for k in range(19))
+
+
+MRT3_M = _d3q19_mrt_rows()
+MRT3_NORM = tuple(float(sum(v * v for v in row)) for row in MRT3_M)
+
+
 def magic_rate(s_nu: float, magic: float = 3.0 / 16.0) -> float:
     """Odd rate for TRT magic parameter Lambda (lattice.py:90-97)."""
     return 1.0 / (0.5 + magic / (1.0 / s_nu - 0.5))
@@ -134,7 +156,17 @@ class Case:
     def mrt_rates(self) -> tuple:
         s_nu = 1.0 / self.tau
         s_q = magic_rate(s_nu, 3.0 / 16.0)  # problem.py:102-106 always uses 3/16
-        return (0.0, self.s_e, self.s_eps, 0.0, s_q, 0.0, s_q, s_nu, s_nu)
+        if self.dim == 2:
+            return (0.0, self.s_e, self.s_eps, 0.0, s_q, 0.0, s_q, s_nu, s_nu)
+        # D3Q19: e -> s_e; eps and the fourth-order pi moments -> s_eps; the energy fluxes q
+        # and the third-order m moments -> s_q; the five shear moments -> 1/tau
+        se, sp = self.s_e, self.s_eps
+        return (0.0, se, sp, 0.0, s_q, 0.0, s_q, 0.0, s_q, s_nu, sp, s_nu, sp, s_nu, s_nu,
+                s_nu, s_q, s_q, s_q)
+
+    def mrt_basis(self) -> tuple:
+        """(M, |M_k|^2) of the lattice's MRT."""
+        return (MRT_M, MRT_NORM) if self.dim == 2 else (MRT3_M, MRT3_NORM)
 
     def force_component(self, a: int) -> Any:
         """Total force along axis a: a float, or an array when a force field is set."""
@@ -342,11 +374,12 @@ def collide(f: list, case: Case, xp: Any = np) -> Any:
             out.append(v)
     elif case.collision == "mrt":
         s = case.mrt_rates()
+        basis, norm = case.mrt_basis()
         dm = []
         for k in range(lat.q):
             acc: Any = 0.0
             for i in range(lat.q):
-                m = float(MRT_M[k][i])
+                m = float(basis[k][i])
                 if m != 0.0:
                     term = -s[k] * m * (f[i] - feq[i])
                     if src is not None:
@@ -356,9 +389,9 @@ def collide(f: list, case: Case, xp: Any = np) -> Any:
         for i in range(lat.q):
             v = f[i]
             for k in range(lat.q):
-                m = float(MRT_M[k][i])
+                m = float(basis[k][i])
                 if m != 0.0:
-                    v = v + (m / MRT_NORM[k]) * dm[k]
+                    v = v + (m / norm[k]) * dm[k]
             out.append(v)
     else:
         raise ValueError(case.collision)

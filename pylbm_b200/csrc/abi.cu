@@ -123,7 +123,7 @@ const char* lbm_error_string(int code) {
         case LBM_OK: return "success";
         case LBM_E_NULL: return "a required pointer is NULL";
         case LBM_E_LATTICE: return "unknown lattice";
-        case LBM_E_COLLISION: return "unknown collision operator (MRT is D2Q9 only)";
+        case LBM_E_COLLISION: return "unknown collision operator";
         case LBM_E_STORAGE: return "unknown storage format";
         case LBM_E_PATTERN: return "unknown streaming pattern";
         case LBM_E_SHAPE: return "invalid lattice shape";
@@ -168,7 +168,6 @@ int lbm_validate(const LbmDesc* d) {
     if (d == nullptr) return LBM_E_NULL;
     if (d->lattice != LBM_D2Q9 && d->lattice != LBM_D3Q19) return LBM_E_LATTICE;
     if (d->collision < LBM_BGK || d->collision > LBM_STREAM_ONLY) return LBM_E_COLLISION;
-    if (d->collision == LBM_MRT && d->lattice != LBM_D2Q9) return LBM_E_COLLISION;
     if (d->storage < LBM_STORE_F32 || d->storage > LBM_STORE_F32_SHIFTED) return LBM_E_STORAGE;
     const int dim = d->lattice == LBM_D2Q9 ? 2 : 3;
     if (d->nx < 1 || d->ny < 1 || d->nz < 1) return LBM_E_SHAPE;

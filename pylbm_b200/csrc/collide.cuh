@@ -400,18 +400,19 @@ __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], f
             f[i] = pi;
             f[o] = po;
         }
-    } else {  // MRT, D2Q9 only (checked on the host)
-        static_assert(L::Q == 9 || COLL != LBM_MRT, "MRT is implemented for D2Q9 only");
-        const float s[9] = {0.0f, r1, r2, 0.0f, r3, 0.0f, r3, r0, r0};
-        float dm[9];
+    } else {  // MRT in moment space with the basis of the lattice (lattice.cuh)
+        const float rate[4] = {r0, r1, r2, r3};
+        float dm[Q];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            // conserved moments (rho, jx, jy) relax with rate 0: only the force term acts
-            const bool conserved = (k == 0 || k == 3 || k == 5);
+        for (int k = 0; k < Q; ++k) {
+            // conserved moments (rho, j) relax with rate 0: only the force term acts
+            const int slot = mrt_rate_slot<L>(k);
+            const bool conserved = slot < 0;
+            const float sk = conserved ? 0.0f : rate[slot < 0 ? 0 : slot];
             float mne = 0.0f, ms = 0.0f;
 #pragma unroll
-            for (int i = 0; i < 9; ++i) {
-                const int m = mrt_m(k, i);
+            for (int i = 0; i < Q; ++i) {
+                const int m = mrt_basis<L>(k, i);
                 if (m != 0) {
                     if (!conserved) mne += float(m) * (f[i] - feq[i]);
                     if (FORCE) ms += float(m) * S[i];
@@ -419,15 +420,17 @@ __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], f
             }
             float num;
             if (conserved) num = FORCE ? ms : 0.0f;
-            else num = FORCE ? -s[k] * mne + (1.0f - 0.5f * s[k]) * ms : -s[k] * mne;
-            dm[k] = num / float(mrt_norm(k));
+            else num = FORCE ? -sk * mne + (1.0f - 0.5f * sk) * ms : -sk * mne;
+            // D2Q9 divides as pylbm's kernel does; D3Q19 multiplies by the folded reciprocal
+            if constexpr (Q == 9) dm[k] = num / float(mrt_basis_norm<L>(k));
+            else dm[k] = num * (1.0f / float(mrt_basis_norm<L>(k)));
         }
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
+        for (int i = 0; i < Q; ++i) {
             float acc = f[i];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                const int m = mrt_m(k, i);
+            for (int k = 0; k < Q; ++k) {
+                const int m = mrt_basis<L>(k, i);
                 if (m != 0) acc += float(m) * dm[k];
             }
             f[i] = acc;

@@ -89,4 +89,92 @@ __host__ __device__ constexpr int mrt_norm(int k) {
     return NRM[k];
 }
 
+// D3Q19 moment basis of d'Humieres et al. (2002), orthogonal, as polynomials of c_i in the
+// velocity order above; rows (rho, e, eps, jx, qx, jy, qy, jz, qz, 3pxx, 3pixx, pww, piww,
+// pxy, pyz, pxz, mx, my, mz). pylbm has no D3Q19 MRT; the rates follow its D2Q9 convention
+// (mrt_rates below).
+__host__ __device__ constexpr int mrt3_poly(int k, int x, int y, int z) {
+    const int c2 = x * x + y * y + z * z;
+    switch (k) {
+        case 0: return 1;
+        case 1: return 19 * c2 - 30;
+        case 2: return (21 * c2 * c2 - 53 * c2 + 24) / 2;
+        case 3: return x;
+        case 4: return (5 * c2 - 9) * x;
+        case 5: return y;
+        case 6: return (5 * c2 - 9) * y;
+        case 7: return z;
+        case 8: return (5 * c2 - 9) * z;
+        case 9: return 3 * x * x - c2;
+        case 10: return (3 * c2 - 5) * (3 * x * x - c2);
+        case 11: return y * y - z * z;
+        case 12: return (3 * c2 - 5) * (y * y - z * z);
+        case 13: return x * y;
+        case 14: return y * z;
+        case 15: return x * z;
+        case 16: return (y * y - z * z) * x;
+        case 17: return (z * z - x * x) * y;
+        default: return (x * x - y * y) * z;
+    }
+}
+struct Mrt3Table {
+    int8_t m[19][19];
+    int16_t norm[19];
+};
+// The table, evaluated by the compiler: inside unrolled loops every entry is an immediate.
+__host__ __device__ constexpr Mrt3Table make_mrt3() {
+    Mrt3Table t{};
+    for (int k = 0; k < 19; ++k) {
+        int n = 0;
+        for (int i = 0; i < 19; ++i) {
+            const int v = mrt3_poly(k, D3Q19::cx(i), D3Q19::cy(i), D3Q19::cz(i));
+            t.m[k][i] = static_cast<int8_t>(v);
+            n += v * v;
+        }
+        t.norm[k] = static_cast<int16_t>(n);
+    }
+    return t;
+}
+__host__ __device__ constexpr int mrt3_m(int k, int i) {
+    constexpr Mrt3Table T = make_mrt3();
+    return T.m[k][i];
+}
+__host__ __device__ constexpr int mrt3_norm(int k) {
+    constexpr Mrt3Table T = make_mrt3();
+    return T.norm[k];
+}
+static_assert(make_mrt3().norm[1] == 2394 && make_mrt3().norm[2] == 252 &&
+                  make_mrt3().norm[10] == 72 && make_mrt3().norm[18] == 8,
+              "d'Humieres et al. (2002) row norms");
+
+// The MRT basis, its squared row norms and the moments it conserves, for either lattice.
+template <class L>
+__host__ __device__ constexpr int mrt_basis(int k, int i) {
+    if constexpr (L::Q == 9) return mrt_m(k, i);
+    else return mrt3_m(k, i);
+}
+template <class L>
+__host__ __device__ constexpr int mrt_basis_norm(int k) {
+    if constexpr (L::Q == 9) return mrt_norm(k);
+    else return mrt3_norm(k);
+}
+template <class L>
+__host__ __device__ constexpr bool mrt_conserved(int k) {
+    return L::Q == 9 ? (k == 0 || k == 3 || k == 5) : (k == 0 || k == 3 || k == 5 || k == 7);
+}
+// Rate of moment k from the descriptor's (r0, r1, r2, r3) = (s_nu, s_e, s_eps, s_q):
+// D2Q9 (0, s_e, s_eps, 0, s_q, 0, s_q, s_nu, s_nu) as pylbm (problem.py:102-106); D3Q19: e ->
+// s_e, eps and the fourth-order pi moments -> s_eps, the energy fluxes q and the third-order
+// m moments -> s_q, the five shear moments -> s_nu.
+template <class L>
+__host__ __device__ constexpr int mrt_rate_slot(int k) {  // 0..3 = r0..r3, -1 = conserved
+    if (mrt_conserved<L>(k)) return -1;
+    if constexpr (L::Q == 9) {
+        return k == 1 ? 1 : k == 2 ? 2 : (k == 4 || k == 6) ? 3 : 0;
+    } else {
+        return k == 1 ? 1 : (k == 2 || k == 10 || k == 12) ? 2
+             : (k == 4 || k == 6 || k == 8 || k >= 16) ? 3 : 0;
+    }
+}
+
 }  // namespace lbm

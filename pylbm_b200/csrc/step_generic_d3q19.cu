@@ -1,4 +1,4 @@
-// Generic kernel instantiations for D3Q19 (BGK, TRT).
+// Generic kernel instantiations for D3Q19 (BGK, TRT, MRT).
 #include "step_generic_inst.cuh"
 
 namespace lbm {
@@ -9,6 +9,7 @@ int launch_generic_d3q19(const LbmDesc& d, const void* src, void* dst, int patte
     switch (d.collision) {
         case LBM_BGK: return go_storage<D3Q19, LBM_BGK>(d, P, src, dst, pattern, s);
         case LBM_TRT: return go_storage<D3Q19, LBM_TRT>(d, P, src, dst, pattern, s);
+        case LBM_MRT: return go_storage<D3Q19, LBM_MRT>(d, P, src, dst, pattern, s);
         case LBM_STREAM_ONLY:
             return go_storage<D3Q19, LBM_STREAM_ONLY>(d, P, src, dst, pattern, s);
     }

@@ -80,8 +80,6 @@ class Box:
         out = []
         if self.collision not in COLLISIONS:
             out.append(f"collision must be one of {COLLISIONS}, got {self.collision!r}")
-        elif self.collision == "mrt" and self.dim != 2:
-            out.append("the MRT collision is defined for D2Q9 only")
         if not self.tau > 0.5:
             out.append(f"tau must exceed 1/2 (positive viscosity), got {self.tau}")
         if self.u_lid != 0.0 and self.periodic[-1]:

@@ -69,9 +69,10 @@ def test_validate_rejects(field, value, code):
 
 
 def test_validate_mrt_3d_lid_periodic_and_index_limit():
+    assert _validate(make_desc(Problem((8, 8, 8), collision="mrt"), 0)) == 0  # D3Q19 MRT
     d = make_desc(Problem((8, 8, 8), collision="trt"), 0)
-    d.collision = _lib.MRT
-    assert _validate(d) == -3
+    d.collision = _lib.MRT  # the TRT descriptor leaves r2, r3 at zero: not MRT rates
+    assert _validate(d) == -8
     d = make_desc(Problem((8, 8), periodic=(True, False), u_lid=0.1), 0)
     d.periodic_mask = 3
     assert _validate(d) == -9
