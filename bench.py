@@ -496,6 +496,7 @@ def extra_single(name: str, f0, peak: float, gpu: int) -> dict:  # noqa: ANN001
     out = entry(s.N, s.bytes_per_node, L, EXTRA_WARMUP, EXTRA_STEPS, dt, clk, peak,
                 dominant_kernel(name))
     out["variant"] = WORKLOADS[name][4]
+    out["roofline"]["traffic"] = traffic_from_profiles(name)
     del s
     free_cuda()
     return out
@@ -516,6 +517,7 @@ def extra_batch(name: str, peak: float, gpu: int) -> dict:
     out = entry(b.nodes, b.bytes_per_node, L, EXTRA_WARMUP, EXTRA_STEPS, dt, clk, peak,
                 "k_d2q9_batch_ab")
     out.update(lattices=len(probs), launch_shape=tune["launch"], variant=BATCHES[name][2])
+    out["roofline"]["traffic"] = traffic_from_profiles(name)
     b.close()
     del b
     free_cuda()

@@ -19,7 +19,8 @@
 // shifted by one element, except at warp edges. The AA scheme is race-free because every
 // memory slot is read and written by one node only (slot (i, x + c_i) belongs to node x); so
 // a lane stores an aligned vector only when all of its elements belong to nodes of its own
-// warp, and the first / last lane stores the slots of its own nodes one element at a time.
+// warp, and the first / last lane stores the V - 1 slots of its own nodes in three aligned
+// pieces (st_tail / st_head in vec.cuh).
 //
 // Semantics are those of the generic kernel (step_generic.cuh) and of pylbm's fused kernel
 // (lbm.cu:71-198, codegen.py:10-16); the collision is the shared collide<>().

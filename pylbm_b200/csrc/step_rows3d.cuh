@@ -204,8 +204,8 @@ k_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
 // A[i, x + c_i] or, behind a wall, to the node's own slot A[opp(i), x] minus the lid term.
 // Every slot is read and written by one node only (slot (i, x + c_i) belongs to node x), so
 // a lane stores an aligned vector only where all its elements belong to nodes of its own
-// warp, which loaded before any lane of the warp stores; the warp-edge lanes store the
-// slots of their own nodes one element at a time.
+// warp, which loaded before any lane of the warp stores; a warp-edge lane stores the V - 1
+// slots of its own nodes in three aligned pieces (st_tail / st_head).
 template <int STORE, int COLL, bool FORCE, bool EDGE>
 __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STORE>::E* A,
                                            const Lane3& l) {
