@@ -5,6 +5,7 @@
 #include "dispatch.cuh"
 #include "staged_launch.cuh"
 #include "step_rows3d.cuh"
+#include "step_staged_rows.cuh"
 
 namespace lbm {
 namespace {
@@ -16,6 +17,12 @@ int go(const StepParams& P, const void* src, void* dst, int pattern, cudaStream_
        bool staged) {
     if (pattern == LBM_PATTERN_AA_EVEN) return go_aa_even<L, STORE, COLL, FORCE>(P, dst, s);
     if (pattern == LBM_PATTERN_AB) {
+        if constexpr (STORE == LBM_STORE_F16 || STORE == LBM_STORE_BF16) {
+            if (staged) {  // whole periodic rows: the row-staged kernel; else the segment one
+                const int rc = go_staged_rows16<STORE, COLL, FORCE>(P, src, dst, s);
+                if (rc != 1) return rc;
+            }
+        }
         if (staged) return go_staged<L, STORE, COLL, FORCE, LBM_PATTERN_AB>(P, src, dst, s);
         return rows3d::go_ab<STORE, COLL, FORCE>(P, src, dst, s);
     }
