@@ -101,7 +101,9 @@ typedef struct LbmDesc {
 
 /* descriptor flags */
 #define LBM_FLAG_GENERIC 1 /* always use the one-node-per-thread kernel (for A/B testing) */
-#define LBM_FLAG_STAGED 2  /* D2Q9: use the TMA-staged kernel instead of the register one */
+#define LBM_FLAG_STAGED 2  /* use the TMA-staged kernels instead of the register ones (D2Q9 and
+                              D3Q19 row segments; 16-bit D3Q19 AB on fully periodic rows of
+                              64..512 nodes: whole staged rows); slower, kept as an option */
 
 /* Library identification. */
 int lbm_abi_version(void);
