@@ -3,7 +3,7 @@
 // Every lane owns V consecutive nodes of one row (16 bytes per plane: 4 fp32 or 8 x 16-bit);
 // the 19 source row segments are read with aligned 16-byte loads at rows (y - c_iy, z - c_iz),
 // shifted along x in registers with one warp shuffle per x-moving plane, and the warp's two
-// halo elements are scalar loads. A block covers several rows when a row has fewer than 128
+// halo elements are scalar loads (none when the warp holds a whole periodic row). A block covers several rows when a row has fewer than 128
 // lanes (block (lanes_x, rows)), so 256-wide rows still fill whole warps; warps never straddle
 // rows. Rows next to a y or z wall take a general path with the wall and lid logic; all other
 // rows run without it (the branch is uniform per warp).
@@ -44,9 +44,13 @@ __device__ __forceinline__ int src_row(const StepParams& P, int y, int z, int cy
     return ys + P.n[1] * zs;
 }
 
+// rot: the warp holds one whole periodic row (nx = 32 V), so the x neighbours across the
+// row's ends are lanes 31 and 0 of the same warp: shifts rotate within the warp, with no halo
+// loads and no partial stores at the row's ends. D3Q19 256^3 (fp16 / bf16) and 128^3 (fp32)
+// measured 0.898 -> 0.923 (AB fp16), 0.825 -> 0.844 (AA fp16), 0.851 -> 0.912 (AA fp32 128^3).
 struct Lane3 {
     int x0, y, z, lane;
-    bool active, first, last;
+    bool active, first, last, rot;
 };
 
 template <int V>
@@ -59,6 +63,7 @@ __device__ __forceinline__ Lane3 lane_of(const StepParams& P) {
     l.active = l.x0 < P.n[0] && l.y < P.n[1];
     l.first = l.lane == 0;
     l.last = l.active && (l.lane == 31 || l.x0 + V >= P.n[0]);
+    l.rot = P.per[0] && P.n[0] == 32 * V;
     return l;
 }
 
@@ -93,12 +98,12 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
         }
         const E* row = A + src_slot * N + r * nx;
         v[i] = NC ? ld_nc(row + l.x0) : ld_plain(row + l.x0);
-        if (cx == 1 && l.first) {
+        if (cx == 1 && l.first && !l.rot) {
             const E* h = l.x0 > 0 ? row + l.x0 - 1
                                   : (P.per[0] ? row + nx - 1 : A + bb_slot * N + own_row * nx);
             halo[i] = NC ? ld1_nc(h) : ld1(h);
         }
-        if (cx == -1 && l.last) {
+        if (cx == -1 && l.last && !l.rot) {
             const E* h = l.x0 + V < nx ? row + l.x0 + V
                                        : (P.per[0] ? row : A + bb_slot * N + own_row * nx + nx - 1);
             halo[i] = NC ? ld1_nc(h) : ld1(h);
@@ -111,12 +116,12 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
         bool wall, top;
         src_row<EDGE>(P, l.y, l.z, L::cy(i), L::cz(i), wall, top);
         if (cx == 1) {
-            uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
-            if (l.first) up = halo[i];
+            uint32_t up = __shfl_sync(kFull, elem<V>(v[i], V - 1), (l.lane + 31) & 31);
+            if (l.first && !l.rot) up = halo[i];
             if (!wall) v[i] = shift_up<V>(v[i], up);
         } else {
-            uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
-            if (l.last) dn = halo[i];
+            uint32_t dn = __shfl_sync(kFull, elem<V>(v[i], 0), (l.lane + 1) & 31);
+            if (l.last && !l.rot) dn = halo[i];
             if (!wall) v[i] = shift_down<V>(v[i], dn);
         }
     }
@@ -124,8 +129,12 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
 
 // Collide the V nodes of the lane in place. With LIDS, lid[i] is added to the pulled value of
 // direction i and sub[i] is subtracted from its post-collision value (the AA-odd push into
-// the lid).
-template <int STORE, int COLL, bool FORCE, bool LIDS>
+// the lid). 16-bit storages: PACK collides the two nodes of a word together with packed f32x2
+// instructions (F2), else one after the other (F1); the results are identical. Under the same
+// 128-register cap (4 blocks per SM) packing measured faster for the pull kernel (D3Q19 256^3
+// TRT AB: fp16 0.923 -> 0.939 of copy, bf16 0.900 -> 0.937) and slower for the AA-odd push
+// kernel, which also holds its push state (fp16 0.844 -> 0.817).
+template <int STORE, int COLL, bool FORCE, bool LIDS, bool PACK>
 __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19],
                                              const float (&lid)[19], const float (&sub)[19]) {
     using T = VT<STORE>;
@@ -144,12 +153,25 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19]
 #pragma unroll
             for (int i = 0; i < 19; ++i) put<V>(v[i], k, T::b(LIDS ? sub_lid(f[i], sub[i]) : f[i]));
         }
+    } else if constexpr (PACK) {  // 16-bit: the two nodes of a word at once
+#pragma unroll
+        for (int jw = 0; jw < 4; ++jw) {
+            F2 f[19];
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                f[i].v = unpack2<STORE>(word(v[i], jw));
+                if (LIDS) f[i] = add_lid(f[i], lid[i]);
+            }
+            collide2<L, COLL, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                if (LIDS) f[i] = sub_lid(f[i], sub[i]);
+                set_word(v[i], jw, pack2<STORE>(f[i].v.x, f[i].v.y));
+            }
+        }
     } else {
         // 16-bit: two nodes per word, packed conversions, the two nodes collided one after the
-        // other (F1 arithmetic, bit-for-bit the packed F2 result). The packed form needs ~45
-        // more registers here (19 populations of two nodes live at once on top of the 76
-        // registers of loaded rows), which drops this latency-bound kernel from 3 to 2
-        // resident blocks per SM: measured 15% slower.
+        // other (F1 arithmetic, bit-for-bit the packed F2 result).
 #pragma unroll
         for (int jw = 0; jw < 4; ++jw) {
             float f0[19], f1[19];
@@ -178,16 +200,17 @@ __device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<ST
     pull_rows<STORE, false, true, EDGE>(P, A, l, v, lid);
     if (!l.active) return;
     const float zero[19] = {};
-    collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid, zero);
+    collide_lane<STORE, COLL, FORCE, EDGE, !FORCE>(P, v, lid, zero);
     const int n0 = (l.y + P.n[1] * l.z) * P.n[0] + l.x0;
 #pragma unroll
     for (int i = 0; i < 19; ++i) st_cs(B + i * P.N + n0, v[i]);
 }
 
-// 16-bit without a body force: capped at 128 registers (4 blocks per SM), which the compiler
-// meets without spills; left free it takes ~158 and 3 blocks, and this latency-bound kernel
-// measured 79.5K instead of 72.5K MLUPS (256^3 TRT fp16). The forced variants would spill
-// several hundred bytes under the cap.
+// 16-bit without a body force: capped at 128 registers (4 blocks per SM), with packed
+// collisions; left free the kernel takes ~158 registers and 3 blocks, and this latency-bound
+// kernel measured 79.5K instead of 72.5K MLUPS (256^3 TRT fp16, one-node collisions). The
+// forced variants would spill several hundred bytes under the cap and keep one-node
+// collisions.
 template <int STORE, int COLL, bool FORCE>
 __global__ void __launch_bounds__(kThreads, (VT<STORE>::V == 8 && !FORCE) ? 4 : 1)
 k_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
@@ -221,7 +244,7 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
         src_row<EDGE>(P, l.y, l.z, -L::cy(i), -L::cz(i), wall, top);
         sub[i] = (wall && top && L::cx(i) != 0) ? lid_term<L>(i, P.ulid) : 0.0f;
     }
-    if (l.active) collide_lane<STORE, COLL, FORCE, EDGE>(P, v, lid, sub);
+    if (l.active) collide_lane<STORE, COLL, FORCE, EDGE, false>(P, v, lid, sub);
     // an opaque zero computed from the collision's output: the push addresses below depend on
     // it, so the compiler forms them after the collision instead of holding all 19 through it.
     // With it the kernel fits 4 blocks per SM (128 registers, 32-40 bytes of spills instead of
@@ -244,22 +267,22 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
         if (cx == 0) {
             if (l.active) st_plain(plane + l.x0, v[i]);
         } else if (cx == 1) {
-            const uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
+            const uint32_t up = __shfl_sync(kFull, elem<V>(v[i], V - 1), (l.lane + 31) & 31);
             if (!l.active) continue;
             const uint4 su = shift_up<V>(v[i], up);
-            if (!l.first) st_plain(plane + l.x0, su);
+            if (!l.first || l.rot) st_plain(plane + l.x0, su);
             else st_tail<V>(plane + l.x0, su);  // slot x0 belongs to the previous warp
-            if (l.last) {
+            if (l.last && !l.rot) {
                 E* dst = l.x0 + V < nx ? plane + l.x0 + V : (P.per[0] ? plane : bb + nx - 1);
                 st1(dst, elem<V>(v[i], V - 1));
             }
         } else {
-            const uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
+            const uint32_t dn = __shfl_sync(kFull, elem<V>(v[i], 0), (l.lane + 1) & 31);
             if (!l.active) continue;
             const uint4 sd = shift_down<V>(v[i], dn);
-            if (!l.last) st_plain(plane + l.x0, sd);
+            if (!l.last || l.rot) st_plain(plane + l.x0, sd);
             else st_head<V>(plane + l.x0, sd);  // slot x0 + V - 1 belongs to the next warp
-            if (l.first) {
+            if (l.first && !l.rot) {
                 E* dst = l.x0 > 0 ? plane + l.x0 - 1 : (P.per[0] ? plane + nx - 1 : bb);
                 st1(dst, elem<V>(v[i], 0));
             }
