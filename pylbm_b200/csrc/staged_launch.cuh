@@ -85,9 +85,10 @@ __global__ void __launch_bounds__(128) k_aa_even(const StepParams P, void* Av) {
         }
     } else {
         // 16-bit: the two nodes of a word collided together with packed f32x2 instructions
-        // (bit-for-bit the one-node result). No register cap: the kernel takes 216 registers
+        // (bit-for-bit the one-node result). No register cap: the kernel takes 255 registers
         // (2 blocks per SM) and keeps 19 loads in flight per thread; capped at 128 it measured
-        // slower (D3Q19 256^3 TRT fp16 AA pair 0.861 -> 0.707 of copy, one-node 0.851 -> 0.813)
+        // slower (D3Q19 256^3 TRT fp16 AA pair 0.861 -> 0.707 of copy, one-node 0.851 -> 0.813),
+        // at 168 (3 blocks) 0.879 -> 0.869, and 8-byte lanes (4 nodes) gained nothing
 #pragma unroll
         for (int jw = 0; jw < 4; ++jw) {
             F2 f[Q];
