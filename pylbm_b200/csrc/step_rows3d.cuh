@@ -2,11 +2,13 @@
 //
 // Every lane owns V consecutive nodes of one row (16 bytes per plane: 4 fp32 or 8 x 16-bit);
 // the 19 source row segments are read with aligned 16-byte loads at rows (y - c_iy, z - c_iz),
-// shifted along x in registers with one warp shuffle per x-moving plane, and the warp's two
-// halo elements are scalar loads (none when the warp holds a whole periodic row). A block covers several rows when a row has fewer than 128
-// lanes (block (lanes_x, rows)), so 256-wide rows still fill whole warps; warps never straddle
-// rows. Rows next to a y or z wall take a general path with the wall and lid logic; all other
-// rows run without it (the branch is uniform per warp).
+// shifted along x in registers with one warp shuffle per x-moving plane, and the two halo
+// elements of a row segment are scalar loads (none when the segment is a whole periodic row).
+// A row of 32 lanes or more spans whole warps (block (lanes_x, rows), lanes_x a multiple of
+// 32); a shorter row takes a power-of-two segment of w lanes and a warp holds 32 / w rows,
+// its shuffles running within segments of width w. Rows next to a y or z wall take a general
+// path with the wall and lid logic; all other rows run without it (the choice is made per
+// warp, so that no shuffle runs in divergent code).
 #pragma once
 
 #include "codec.cuh"
@@ -44,32 +46,50 @@ __device__ __forceinline__ int src_row(const StepParams& P, int y, int z, int cy
     return ys + P.n[1] * zs;
 }
 
-// rot: the warp holds one whole periodic row (nx = 32 V), so the x neighbours across the
-// row's ends are lanes 31 and 0 of the same warp: shifts rotate within the warp, with no halo
-// loads and no partial stores at the row's ends. D3Q19 256^3 (fp16 / bf16) and 128^3 (fp32)
-// measured 0.898 -> 0.923 (AB fp16), 0.825 -> 0.844 (AA fp16), 0.851 -> 0.912 (AA fp32 128^3).
+// w: lanes of a row segment (32, or the power of two a shorter row is given); sl: the lane's
+// index in it. rot: the segment holds one whole periodic row (nx = w V), so the x neighbours
+// across the row's ends are its last and first lanes: shifts rotate within the segment, with
+// no halo loads and no partial stores at the row's ends. D3Q19 256^3 (fp16 / bf16) and 128^3
+// (fp32) measured 0.898 -> 0.923 (AB fp16), 0.825 -> 0.844 (AA fp16), 0.851 -> 0.912 (AA fp32
+// 128^3).
 struct Lane3 {
-    int x0, y, z, lane;
+    int x0, y, z, sl, w;
     bool active, first, last, rot;
 };
 
 template <int V>
 __device__ __forceinline__ Lane3 lane_of(const StepParams& P) {
     Lane3 l;
-    l.lane = threadIdx.x & 31;
+    l.w = blockDim.x < 32 ? int(blockDim.x) : 32;
+    l.sl = threadIdx.x & (l.w - 1);
     l.x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
     l.y = blockIdx.y * blockDim.y + threadIdx.y;
     l.z = blockIdx.z;
     l.active = l.x0 < P.n[0] && l.y < P.n[1];
-    l.first = l.lane == 0;
-    l.last = l.active && (l.lane == 31 || l.x0 + V >= P.n[0]);
-    l.rot = P.per[0] && P.n[0] == 32 * V;
+    l.first = l.sl == 0;
+    l.last = l.active && (l.sl == l.w - 1 || l.x0 + V >= P.n[0]);
+    l.rot = P.per[0] && P.n[0] == l.w * V;
     return l;
+}
+
+// The value of lane sl - 1 (up) or sl + 1 (dn) of the segment, cyclically.
+__device__ __forceinline__ uint32_t from_prev(const Lane3& l, uint32_t x) {
+    return __shfl_sync(kFull, x, (l.sl + l.w - 1) & (l.w - 1), l.w);
+}
+__device__ __forceinline__ uint32_t from_next(const Lane3& l, uint32_t x) {
+    return __shfl_sync(kFull, x, (l.sl + 1) & (l.w - 1), l.w);
 }
 
 __device__ __forceinline__ bool edge_row(const StepParams& P, int y, int z) {
     return (!P.per[1] && (y == 0 || y == P.n[1] - 1)) ||
            (!P.per[2] && (z == 0 || z == P.n[2] - 1));
+}
+
+// Whether the warp takes the wall path: any of its rows is next to a y or z wall (all 32 lanes
+// call this, before any of them can leave).
+__device__ __forceinline__ bool edge_warp(const StepParams& P, const Lane3& l) {
+    const bool e = edge_row(P, l.y, l.z);
+    return l.w < 32 ? __any_sync(kFull, e) : e;
 }
 
 template <int STORE, bool READ_OPP, bool NC, bool EDGE>
@@ -116,11 +136,11 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
         bool wall, top;
         src_row<EDGE>(P, l.y, l.z, L::cy(i), L::cz(i), wall, top);
         if (cx == 1) {
-            uint32_t up = __shfl_sync(kFull, elem<V>(v[i], V - 1), (l.lane + 31) & 31);
+            uint32_t up = from_prev(l, elem<V>(v[i], V - 1));
             if (l.first && !l.rot) up = halo[i];
             if (!wall) v[i] = shift_up<V>(v[i], up);
         } else {
-            uint32_t dn = __shfl_sync(kFull, elem<V>(v[i], 0), (l.lane + 1) & 31);
+            uint32_t dn = from_next(l, elem<V>(v[i], 0));
             if (l.last && !l.rot) dn = halo[i];
             if (!wall) v[i] = shift_down<V>(v[i], dn);
         }
@@ -218,7 +238,7 @@ k_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
     const E* __restrict__ A = static_cast<const E*>(Av);
     E* __restrict__ B = static_cast<E*>(Bv);
     const Lane3 l = lane_of<VT<STORE>::V>(P);
-    if (edge_row(P, l.y, l.z)) ab_row<STORE, COLL, FORCE, true>(P, A, B, l);
+    if (edge_warp(P, l)) ab_row<STORE, COLL, FORCE, true>(P, A, B, l);
     else ab_row<STORE, COLL, FORCE, false>(P, A, B, l);
 }
 
@@ -267,7 +287,7 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
         if (cx == 0) {
             if (l.active) st_plain(plane + l.x0, v[i]);
         } else if (cx == 1) {
-            const uint32_t up = __shfl_sync(kFull, elem<V>(v[i], V - 1), (l.lane + 31) & 31);
+            const uint32_t up = from_prev(l, elem<V>(v[i], V - 1));
             if (!l.active) continue;
             const uint4 su = shift_up<V>(v[i], up);
             if (!l.first || l.rot) st_plain(plane + l.x0, su);
@@ -277,7 +297,7 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
                 st1(dst, elem<V>(v[i], V - 1));
             }
         } else {
-            const uint32_t dn = __shfl_sync(kFull, elem<V>(v[i], 0), (l.lane + 1) & 31);
+            const uint32_t dn = from_next(l, elem<V>(v[i], 0));
             if (!l.active) continue;
             const uint4 sd = shift_down<V>(v[i], dn);
             if (!l.last || l.rot) st_plain(plane + l.x0, sd);
@@ -296,13 +316,19 @@ k_aa_odd(const StepParams P, void* Av) {
     using E = typename VT<STORE>::E;
     E* A = static_cast<E*>(Av);
     const Lane3 l = lane_of<VT<STORE>::V>(P);
-    if (edge_row(P, l.y, l.z)) aa_odd_row<STORE, COLL, FORCE, true>(P, A, l);
+    if (edge_warp(P, l)) aa_odd_row<STORE, COLL, FORCE, true>(P, A, l);
     else aa_odd_row<STORE, COLL, FORCE, false>(P, A, l);
 }
 
 // Block shape (lanes along x, rows) for rows of nx nodes.
 inline dim3 block_for_rows(int nx, int V) {
-    int lanes = (nx / V + 31) / 32 * 32;
+    const int need = (nx + V - 1) / V;
+    if (need < 32) {  // a power-of-two segment per row, 32 / w rows per warp
+        int w = 1;
+        while (w < need) w <<= 1;
+        return dim3(w, kThreads / w);
+    }
+    int lanes = (need + 31) / 32 * 32;
     if (lanes > kThreads) lanes = kThreads;
     return dim3(lanes, kThreads / lanes);
 }

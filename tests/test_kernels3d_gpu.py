@@ -138,3 +138,36 @@ def test_d3q19_row_staged_kernel_matches_generic(variant, coll, force, nx):
         s.step(12)
     assert _lib.device_error() == 0
     assert np.array_equal(a.populations(), g.populations())
+
+
+@pytest.mark.parametrize("variant", ["fused", "fused-fp16", "fused-aa", "fused-aa-bf16"])
+@pytest.mark.parametrize("shape,extra", [
+    # rows shorter than a warp share it in power-of-two segments: whole periodic rows (fp16
+    # 16 lanes, fp32 32), walls on every axis (8 / 16 lanes; a warp holds rows next to a wall
+    # and rows that are not), partial segments (5 of 8 / 10 of 16 lanes) with a force
+    ((128, 12, 9), {"collision": "trt", "periodic": (True, True, True)}),
+    ((64, 12, 9), {"collision": "bgk", "u_lid": 0.06}),
+    ((40, 12, 9), {"collision": "trt", "periodic": (True, False, False),
+                   "force": (1e-5, 0.0, -2e-5)}),
+    ((8, 20, 9), {"collision": "bgk", "periodic": (True, True, False), "u_lid": 0.05}),
+])
+def test_d3q19_short_rows_match_generic(variant, shape, extra):
+    """The register row kernels on rows of fewer than 32 lanes give the generic kernel's
+    result (bit for bit in 16-bit storage)."""
+    from pylbm_b200 import _lib
+    from pylbm_b200.backend import VARIANTS
+    from pylbm_b200.problem import Problem
+
+    p = Problem(shape, tau=0.57, **extra)
+    f0 = _smooth_state(p)
+    a, g = VARIANTS[variant](p), VARIANTS[variant](p)
+    g.desc.flags = _lib.FLAG_GENERIC
+    for s in (a, g):
+        s.set_populations(f0)
+        s.step(12)
+    assert _lib.device_error() == 0
+    if a.storage == "f32":
+        diff = np.abs(a.populations() - g.populations()).max()
+        assert diff < 1e-6, diff
+    else:
+        assert np.array_equal(a.populations(), g.populations())
