@@ -400,7 +400,79 @@ __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], f
             f[i] = pi;
             f[o] = po;
         }
-    } else {  // MRT in moment space with the basis of the lattice (lattice.cuh)
+    } else if constexpr (Q == 19) {
+        // D3Q19 MRT in moment space (d'Humieres et al. 2002 basis, lattice.cuh). Every basis
+        // row is even or odd under c -> -c, so the moments of g = f - feq (and of S) come from
+        // the 9 pair sums g_i + g_opp and the 9 pair differences g_i - g_opp, and the update
+        // f += M^T dm is formed once per pair as f_i += E + O, f_opp += E - O (E from the even
+        // moments, O from the odd ones): half the multiply-adds of the full 19 x 19 products,
+        // the same algebra.
+        const float rate[4] = {r0, r1, r2, r3};
+        const float g0 = f[0] - feq[0];
+        float ga[Q], gd[Q], sa[Q], sd[Q];  // indexed by the pair's leading direction
+#pragma unroll
+        for (int i = 1; i < Q; ++i) {
+            if (!leads_pair<L>(i)) continue;
+            const int o = L::opp(i);
+            const float gi = f[i] - feq[i], go = f[o] - feq[o];
+            ga[i] = gi + go;
+            gd[i] = gi - go;
+            if (FORCE) {
+                sa[i] = S[i] + S[o];
+                sd[i] = S[i] - S[o];
+            }
+        }
+        float dm[Q];
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            const int slot = mrt_rate_slot<L>(k);
+            const bool conserved = slot < 0;
+            const float sk = conserved ? 0.0f : rate[slot < 0 ? 0 : slot];
+            const bool even = mrt_parity<L>(k) > 0;
+            float mne = 0.0f, ms = 0.0f;
+            if (even) {
+                const int m0 = mrt_basis<L>(k, 0);
+                if (m0 != 0) {
+                    if (!conserved) mne = float(m0) * g0;
+                    if (FORCE) ms = float(m0) * S[0];
+                }
+            }
+#pragma unroll
+            for (int i = 1; i < Q; ++i) {
+                if (!leads_pair<L>(i)) continue;
+                const int m = mrt_basis<L>(k, i);
+                if (m == 0) continue;
+                if (!conserved) mne += float(m) * (even ? ga[i] : gd[i]);
+                if (FORCE) ms += float(m) * (even ? sa[i] : sd[i]);
+            }
+            float num;
+            if (conserved) num = FORCE ? ms : 0.0f;
+            else num = FORCE ? -sk * mne + (1.0f - 0.5f * sk) * ms : -sk * mne;
+            dm[k] = num * (1.0f / float(mrt_basis_norm<L>(k)));
+        }
+        float e0 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            const int m0 = mrt_basis<L>(k, 0);
+            if (m0 != 0) e0 += float(m0) * dm[k];
+        }
+        f[0] += e0;
+#pragma unroll
+        for (int i = 1; i < Q; ++i) {
+            if (!leads_pair<L>(i)) continue;
+            const int o = L::opp(i);
+            float E = 0.0f, O = 0.0f;
+#pragma unroll
+            for (int k = 0; k < Q; ++k) {
+                const int m = mrt_basis<L>(k, i);
+                if (m == 0) continue;
+                if (mrt_parity<L>(k) > 0) E += float(m) * dm[k];
+                else O += float(m) * dm[k];
+            }
+            f[i] += E + O;
+            f[o] += E - O;
+        }
+    } else {  // D2Q9 MRT in moment space with the basis of lattice.cuh, as pylbm's kernel
         const float rate[4] = {r0, r1, r2, r3};
         float dm[Q];
 #pragma unroll
@@ -421,9 +493,7 @@ __device__ __forceinline__ void collide(float (&f)[L::Q], const float (&F)[3], f
             float num;
             if (conserved) num = FORCE ? ms : 0.0f;
             else num = FORCE ? -sk * mne + (1.0f - 0.5f * sk) * ms : -sk * mne;
-            // D2Q9 divides as pylbm's kernel does; D3Q19 multiplies by the folded reciprocal
-            if constexpr (Q == 9) dm[k] = num / float(mrt_basis_norm<L>(k));
-            else dm[k] = num * (1.0f / float(mrt_basis_norm<L>(k)));
+            dm[k] = num / float(mrt_basis_norm<L>(k));  // a division, as pylbm's kernel
         }
 #pragma unroll
         for (int i = 0; i < Q; ++i) {

@@ -32,6 +32,9 @@ int launch_fast_d2q9(const LbmDesc& d, const void* src, void* dst, int pattern,
                      cudaStream_t s);
 int launch_fast_d3q19(const LbmDesc& d, const void* src, void* dst, int pattern,
                       cudaStream_t s);
+// D3Q19 MRT on the register row kernels (step_d3q19_mrt.cu), for descriptors that
+// launch_fast_d3q19 accepts.
+int launch_mrt_d3q19(const LbmDesc& d, const void* src, void* dst, int pattern, cudaStream_t s);
 
 // One lattice of a batch (device table entry, batched.cu / step_d2q9.cu).
 struct BatchLattice {

@@ -120,6 +120,7 @@ __host__ __device__ constexpr int mrt3_poly(int k, int x, int y, int z) {
 struct Mrt3Table {
     int8_t m[19][19];
     int16_t norm[19];
+    int8_t parity[19];  // +1: M[k][opp(i)] = M[k][i] for all i; -1: = -M[k][i]; 0: neither
 };
 // The table, evaluated by the compiler: inside unrolled loops every entry is an immediate.
 __host__ __device__ constexpr Mrt3Table make_mrt3() {
@@ -133,6 +134,14 @@ __host__ __device__ constexpr Mrt3Table make_mrt3() {
         }
         t.norm[k] = static_cast<int16_t>(n);
     }
+    for (int k = 0; k < 19; ++k) {
+        bool even = true, odd = true;
+        for (int i = 0; i < 19; ++i) {
+            even = even && t.m[k][i] == t.m[k][D3Q19::opp(i)];
+            odd = odd && t.m[k][i] == -t.m[k][D3Q19::opp(i)];
+        }
+        t.parity[k] = static_cast<int8_t>(even ? 1 : (odd ? -1 : 0));
+    }
     return t;
 }
 __host__ __device__ constexpr int mrt3_m(int k, int i) {
@@ -142,6 +151,10 @@ __host__ __device__ constexpr int mrt3_m(int k, int i) {
 __host__ __device__ constexpr int mrt3_norm(int k) {
     constexpr Mrt3Table T = make_mrt3();
     return T.norm[k];
+}
+__host__ __device__ constexpr int mrt3_parity(int k) {
+    constexpr Mrt3Table T = make_mrt3();
+    return T.parity[k];
 }
 static_assert(make_mrt3().norm[1] == 2394 && make_mrt3().norm[2] == 252 &&
                   make_mrt3().norm[10] == 72 && make_mrt3().norm[18] == 8,
@@ -162,6 +175,33 @@ template <class L>
 __host__ __device__ constexpr bool mrt_conserved(int k) {
     return L::Q == 9 ? (k == 0 || k == 3 || k == 5) : (k == 0 || k == 3 || k == 5 || k == 7);
 }
+// Parity of basis row k under c -> -c: +1 when M[k][opp(i)] = M[k][i] for every i (even
+// moments: they see only the pair sums f_i + f_opp(i)), -1 when M[k][opp(i)] = -M[k][i] (odd
+// moments: pair differences), 0 for a row that is neither. D3Q19 reads it from the table the
+// compiler evaluates (a loop here, left to the optimiser inside unrolled code, kept the table
+// in local memory).
+template <class L>
+__host__ __device__ constexpr int mrt_parity(int k) {
+    if constexpr (L::Q == 19) {
+        return mrt3_parity(k);
+    } else {
+        bool even = true, odd = true;
+        for (int i = 0; i < L::Q; ++i) {
+            const int a = mrt_basis<L>(k, i), b = mrt_basis<L>(k, L::opp(i));
+            even = even && a == b;
+            odd = odd && a == -b;
+        }
+        return even ? 1 : (odd ? -1 : 0);
+    }
+}
+template <class L>
+__host__ __device__ constexpr bool mrt_rows_have_parity() {
+    for (int k = 0; k < L::Q; ++k)
+        if (mrt_parity<L>(k) == 0) return false;
+    return true;
+}
+static_assert(mrt_rows_have_parity<D3Q19>(), "every D3Q19 basis row is even or odd");
+
 // Rate of moment k from the descriptor's (r0, r1, r2, r3) = (s_nu, s_e, s_eps, s_q):
 // D2Q9 (0, s_e, s_eps, 0, s_q, 0, s_q, s_nu, s_nu) as pylbm (problem.py:102-106); D3Q19: e ->
 // s_e, eps and the fourth-order pi moments -> s_eps, the energy fluxes q and the third-order

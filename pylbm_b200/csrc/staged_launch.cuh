@@ -73,7 +73,17 @@ __global__ void __launch_bounds__(128) k_aa_even(const StepParams P, void* Av) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) v[i] = ld_plain(A + i * P.N + n0);
     const float F[3] = {P.F[0], P.F[1], P.F[2]};
-    if constexpr (V == 4) {
+    if constexpr (COLL == LBM_MRT) {  // one copy of the moment transform (step_rows3d.cuh)
+#pragma unroll 1
+        for (int k = 0; k < V; ++k) {
+            float f[Q];
+#pragma unroll
+            for (int i = 0; i < Q; ++i) f[i] = T::f(elem<V>(v[i], 0));
+            collide<L, COLL, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+            for (int i = 0; i < Q; ++i) v[i] = shift_down<V>(v[i], T::b(f[i]));
+        }
+    } else if constexpr (V == 4) {
 #pragma unroll
         for (int k = 0; k < V; ++k) {
             float f[Q];

@@ -44,10 +44,9 @@ int go_c(const LbmDesc& d, const StepParams& P, const void* src, void* dst, int 
     switch (d.collision) {
         case LBM_BGK: return go_f<STORE, LBM_BGK>(d, P, src, dst, pattern, s);
         case LBM_TRT: return go_f<STORE, LBM_TRT>(d, P, src, dst, pattern, s);
-        // MRT: the generic kernel (one node per thread). The row kernels collide 4-8 nodes
-        // per lane, and 8 unrolled copies of the 19 x 19 moment transform made one
-        // translation unit take half an hour to compile
-        case LBM_MRT: return 1;
+        // MRT: the register row kernels with a rolled node loop, in a translation unit of
+        // their own (step_d3q19_mrt.cu); no TMA-staged form
+        case LBM_MRT: return launch_mrt_d3q19(d, src, dst, pattern, s);
         case LBM_STREAM_ONLY:
             return go<STORE, LBM_STREAM_ONLY, false>(P, src, dst, pattern, s,
                                                      (d.flags & LBM_FLAG_STAGED) != 0);

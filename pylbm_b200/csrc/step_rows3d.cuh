@@ -160,7 +160,25 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[19]
     using T = VT<STORE>;
     constexpr int V = T::V;
     const float F[3] = {P.F[0], P.F[1], P.F[2]};
-    if constexpr (V == 4) {
+    if constexpr (COLL == LBM_MRT) {
+        // One copy of the moment transform per kernel (8 unrolled copies made one translation
+        // unit take half an hour to compile): a rolled loop over the lane's nodes collides
+        // element 0 and rotates every vector down by one element, appending the result, so
+        // after V passes each result sits in its node's place.
+#pragma unroll 1
+        for (int k = 0; k < V; ++k) {
+            float f[19];
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                f[i] = T::f(elem<V>(v[i], 0));
+                if (LIDS) f[i] = add_lid(f[i], lid[i]);
+            }
+            collide<L, LBM_MRT, Codec<STORE>::shifted, FORCE>(f, F, P.r0, P.r1, P.r2, P.r3);
+#pragma unroll
+            for (int i = 0; i < 19; ++i)
+                v[i] = shift_down<V>(v[i], T::b(LIDS ? sub_lid(f[i], sub[i]) : f[i]));
+        }
+    } else if constexpr (V == 4) {
 #pragma unroll
         for (int k = 0; k < V; ++k) {
             float f[19];
@@ -232,7 +250,8 @@ __device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<ST
 // forced variants would spill several hundred bytes under the cap and keep one-node
 // collisions.
 template <int STORE, int COLL, bool FORCE>
-__global__ void __launch_bounds__(kThreads, (VT<STORE>::V == 8 && !FORCE) ? 4 : 1)
+__global__ void __launch_bounds__(kThreads,
+                                  (VT<STORE>::V == 8 && !FORCE && COLL != LBM_MRT) ? 4 : 1)
 k_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
     using E = typename VT<STORE>::E;
     const E* __restrict__ A = static_cast<const E*>(Av);
@@ -311,7 +330,7 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
 }
 
 template <int STORE, int COLL, bool FORCE>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, COLL == LBM_MRT ? 1 : 4)
 k_aa_odd(const StepParams P, void* Av) {
     using E = typename VT<STORE>::E;
     E* A = static_cast<E*>(Av);
