@@ -248,7 +248,11 @@ def test_mass_and_momentum_drift_fp64():
 # ----------------------------------------------------------------------------- fast paths
 # Row widths that give several warps and a partial last warp for 4- and 8-wide lanes.
 FAST_SHAPES = [((264, 7), (True, True)), ((264, 7), (False, False)), ((520, 5), (True, False)),
-               ((136, 9), (False, True)), ((1032, 4), (False, False))]
+               ((136, 9), (False, True)), ((1032, 4), (False, False)),
+               # rows of fewer than 32 lanes share a warp in power-of-two segments: whole
+               # periodic rows, walls, partial segments, one- and two-lane rows
+               ((128, 6), (True, True)), ((64, 9), (False, False)), ((40, 7), (True, False)),
+               ((8, 11), (True, True)), ((24, 5), (False, True))]
 STORAGES = {"f32": (0, np.float32), "f32s": (3, np.float32), "f16": (1, np.float16),
             "bf16": (2, "bf16")}
 
@@ -319,6 +323,41 @@ def test_fast_matches_generic_kernel(variant, coll, extra):
     for s in (a, g):
         s.set_populations(f0)
         s.step(40)
+    if a.storage == "f32":
+        diff = np.abs(a.populations() - g.populations()).max()
+        assert diff < 1e-6, diff
+    else:
+        assert np.array_equal(a.populations(), g.populations())
+
+
+@pytest.mark.parametrize("variant", ["fused", "fused-aa", "fused-fp16", "fused-aa-bf16"])
+@pytest.mark.parametrize("shape,coll,extra", [
+    ((128, 40), "trt", {"periodic": (True, True)}),
+    ((64, 40), "bgk", {"u_lid": 0.08}),
+    ((40, 30), "trt", {"force": (2e-5, -1e-5), "periodic": (True, False)}),
+    ((8, 40), "mrt", {"u_lid": 0.05, "periodic": (True, False)}),
+])
+def test_fast_short_rows_match_generic_kernel(variant, shape, coll, extra):
+    """Rows of fewer than 32 lanes (warp segments, rotation for whole periodic rows) give the
+    one-node-per-thread kernel's result: bit for bit in 16-bit storage, within 1e-6 in fp32."""
+    from pylbm_b200 import _lib
+    from pylbm_b200.problem import Problem
+
+    B = _backend()
+    p = Problem(shape, tau=0.62, collision=coll, **extra)
+    rng = np.random.default_rng(5)
+    rho = 1.0 + 0.01 * rng.standard_normal(p.array_shape)
+    u = 0.04 * (rng.random((2,) + p.array_shape) - 0.5)
+    from pylbm_b200.lattice import equilibrium
+
+    f0 = equilibrium(p.lattice, rho, u)
+    a = B.VARIANTS[variant](p)
+    g = B.VARIANTS[variant](p)
+    g.desc.flags = _lib.FLAG_GENERIC
+    for s in (a, g):
+        s.set_populations(f0)
+        s.step(40)
+    assert _lib.device_error() == 0
     if a.storage == "f32":
         diff = np.abs(a.populations() - g.populations()).max()
         assert diff < 1e-6, diff
