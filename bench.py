@@ -67,6 +67,10 @@ WORKLOADS = {
     "d3q19-trt-aa-f32": ("D3Q19", 256, "trt", 0.55, "fused-aa"),
     "d3q19-trt-aa-f16": ("D3Q19", 256, "trt", 0.55, "fused-aa-fp16"),
     "d3q19-trt-aa-bf16": ("D3Q19", 256, "trt", 0.55, "fused-aa-bf16"),
+    # d'Humieres et al. (2002) MRT (no pylbm counterpart)
+    "d3q19-mrt-ab-f32": ("D3Q19", 256, "mrt", 0.55, "fused"),
+    "d3q19-mrt-ab-f16": ("D3Q19", 256, "mrt", 0.55, "fused-fp16"),
+    "d3q19-mrt-aa-f16": ("D3Q19", 256, "mrt", 0.55, "fused-aa-fp16"),
     # lid-driven cavities (walls on every axis, lid U = 0.05 on the top of the last axis)
     "d2q9-bgk-cavity-f32": ("D2Q9", 4096, "bgk", 0.6, "fused"),
     "d2q9-mrt-cavity-f32": ("D2Q9", 4096, "mrt", 0.6, "fused"),

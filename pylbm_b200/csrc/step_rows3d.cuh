@@ -57,10 +57,13 @@ struct Lane3 {
     bool active, first, last, rot;
 };
 
-template <int V>
+// SEG: the block may hold rows of fewer than 32 lanes (w from the block shape); otherwise w is
+// the constant 32 and the shuffles compile to their whole-warp form (the runtime width cost
+// ~1.3 % at 256^3 fp16, where every row spans whole warps).
+template <int V, bool SEG>
 __device__ __forceinline__ Lane3 lane_of(const StepParams& P) {
     Lane3 l;
-    l.w = blockDim.x < 32 ? int(blockDim.x) : 32;
+    l.w = (SEG && blockDim.x < 32) ? int(blockDim.x) : 32;
     l.sl = threadIdx.x & (l.w - 1);
     l.x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
     l.y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -87,9 +90,11 @@ __device__ __forceinline__ bool edge_row(const StepParams& P, int y, int z) {
 
 // Whether the warp takes the wall path: any of its rows is next to a y or z wall (all 32 lanes
 // call this, before any of them can leave).
+template <bool SEG>
 __device__ __forceinline__ bool edge_warp(const StepParams& P, const Lane3& l) {
     const bool e = edge_row(P, l.y, l.z);
-    return l.w < 32 ? __any_sync(kFull, e) : e;
+    if constexpr (SEG) return l.w < 32 ? __any_sync(kFull, e) : e;
+    else return e;
 }
 
 template <int STORE, bool READ_OPP, bool NC, bool EDGE>
@@ -249,15 +254,15 @@ __device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<ST
 // kernel measured 79.5K instead of 72.5K MLUPS (256^3 TRT fp16, one-node collisions). The
 // forced variants would spill several hundred bytes under the cap and keep one-node
 // collisions.
-template <int STORE, int COLL, bool FORCE>
+template <int STORE, int COLL, bool FORCE, bool SEG>
 __global__ void __launch_bounds__(kThreads,
                                   (VT<STORE>::V == 8 && !FORCE && COLL != LBM_MRT) ? 4 : 1)
 k_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
     using E = typename VT<STORE>::E;
     const E* __restrict__ A = static_cast<const E*>(Av);
     E* __restrict__ B = static_cast<E*>(Bv);
-    const Lane3 l = lane_of<VT<STORE>::V>(P);
-    if (edge_warp(P, l)) ab_row<STORE, COLL, FORCE, true>(P, A, B, l);
+    const Lane3 l = lane_of<VT<STORE>::V, SEG>(P);
+    if (edge_warp<SEG>(P, l)) ab_row<STORE, COLL, FORCE, true>(P, A, B, l);
     else ab_row<STORE, COLL, FORCE, false>(P, A, B, l);
 }
 
@@ -329,20 +334,21 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
     }
 }
 
-template <int STORE, int COLL, bool FORCE>
+template <int STORE, int COLL, bool FORCE, bool SEG>
 __global__ void __launch_bounds__(kThreads, COLL == LBM_MRT ? 1 : 4)
 k_aa_odd(const StepParams P, void* Av) {
     using E = typename VT<STORE>::E;
     E* A = static_cast<E*>(Av);
-    const Lane3 l = lane_of<VT<STORE>::V>(P);
-    if (edge_warp(P, l)) aa_odd_row<STORE, COLL, FORCE, true>(P, A, l);
+    const Lane3 l = lane_of<VT<STORE>::V, SEG>(P);
+    if (edge_warp<SEG>(P, l)) aa_odd_row<STORE, COLL, FORCE, true>(P, A, l);
     else aa_odd_row<STORE, COLL, FORCE, false>(P, A, l);
 }
 
-// Block shape (lanes along x, rows) for rows of nx nodes.
-inline dim3 block_for_rows(int nx, int V) {
+// Block shape (lanes along x, rows) for rows of nx nodes; SEG: rows of fewer than 32 lanes take
+// power-of-two segments of a warp (else a whole warp, the rest of it idle).
+inline dim3 block_for_rows(int nx, int V, bool seg) {
     const int need = (nx + V - 1) / V;
-    if (need < 32) {  // a power-of-two segment per row, 32 / w rows per warp
+    if (seg && need < 32) {  // a power-of-two segment per row, 32 / w rows per warp
         int w = 1;
         while (w < need) w <<= 1;
         return dim3(w, kThreads / w);
@@ -352,23 +358,36 @@ inline dim3 block_for_rows(int nx, int V) {
     return dim3(lanes, kThreads / lanes);
 }
 
+// Whether a launch takes the segmented kernel: rows of fewer than 32 lanes, and every MRT or
+// forced launch (those are compute-bound and keep one instantiation).
+template <int COLL, bool FORCE>
+inline bool use_seg(int nx, int V) {
+    return COLL == LBM_MRT || FORCE || (nx + V - 1) / V < 32;
+}
+
 template <int STORE, int COLL, bool FORCE>
 int go_ab(const StepParams& P, const void* src, void* dst, cudaStream_t s) {
     constexpr int V = VT<STORE>::V;
-    const dim3 block = block_for_rows(P.n[0], V);
+    constexpr bool kOnlySeg = COLL == LBM_MRT || FORCE;
+    const bool seg = use_seg<COLL, FORCE>(P.n[0], V);
+    const dim3 block = block_for_rows(P.n[0], V, seg);
     const dim3 grid((P.n[0] / V + block.x - 1) / block.x, (P.n[1] + block.y - 1) / block.y,
                     P.n[2]);
-    k_ab<STORE, COLL, FORCE><<<grid, block, 0, s>>>(P, src, dst);
+    if (seg || kOnlySeg) k_ab<STORE, COLL, FORCE, true><<<grid, block, 0, s>>>(P, src, dst);
+    else k_ab<STORE, COLL, FORCE, kOnlySeg><<<grid, block, 0, s>>>(P, src, dst);
     return int(cudaGetLastError());
 }
 
 template <int STORE, int COLL, bool FORCE>
 int go_aa_odd(const StepParams& P, void* buf, cudaStream_t s) {
     constexpr int V = VT<STORE>::V;
-    const dim3 block = block_for_rows(P.n[0], V);
+    constexpr bool kOnlySeg = COLL == LBM_MRT || FORCE;
+    const bool seg = use_seg<COLL, FORCE>(P.n[0], V);
+    const dim3 block = block_for_rows(P.n[0], V, seg);
     const dim3 grid((P.n[0] / V + block.x - 1) / block.x, (P.n[1] + block.y - 1) / block.y,
                     P.n[2]);
-    k_aa_odd<STORE, COLL, FORCE><<<grid, block, 0, s>>>(P, buf);
+    if (seg || kOnlySeg) k_aa_odd<STORE, COLL, FORCE, true><<<grid, block, 0, s>>>(P, buf);
+    else k_aa_odd<STORE, COLL, FORCE, kOnlySeg><<<grid, block, 0, s>>>(P, buf);
     return int(cudaGetLastError());
 }
 
