@@ -103,7 +103,8 @@ typedef struct LbmDesc {
 #define LBM_FLAG_GENERIC 1 /* always use the one-node-per-thread kernel (for A/B testing) */
 #define LBM_FLAG_STAGED 2  /* use the TMA-staged kernels instead of the register ones (D2Q9 and
                               D3Q19 row segments; 16-bit D3Q19 AB on fully periodic rows of
-                              64..512 nodes: whole staged rows); slower, kept as an option */
+                              64..512 nodes: whole staged rows; D3Q19 MRT has no staged form
+                              and ignores it); slower, kept as an option */
 
 /* Library identification. */
 int lbm_abi_version(void);
