@@ -7,12 +7,16 @@
 // shuffle. Only the first and last lane of a warp read one more element (the warp's halo) with
 // a scalar load that the neighbouring warp's line already brought into L2; warps are
 // otherwise independent (no shared memory, no block barrier). x walls and the periodic x wrap
-// are resolved inside that halo element.
+// are resolved inside that halo element. Rows of fewer than 128 lanes run a second form of the
+// kernels (SEG) with several rows per block: a row of fewer than 32 lanes takes a power-of-two
+// segment of a warp (32 / w rows per warp, shuffles of width w), and a segment that holds a
+// whole periodic row rotates its shifts within itself (no halo loads, no partial stores).
+// Longer rows keep one row per block (see lane_of).
 //
 // Rows next to a y wall (y = 0 and y = ny - 1 of a non-periodic y axis) take a separate,
 // general code path (the whole segment bounces back from the node's own opposite plane, plus
 // the lid term on the top wall); every other row runs a path with no wall or lid code at all.
-// The branch is uniform per block, and keeping the wall logic out of the hot path keeps its
+// The branch is uniform per warp, and keeping the wall logic out of the hot path keeps its
 // nine loads in flight together (measured: the fused variant ran 20% slower otherwise).
 //
 // AA-odd push: the write of p_i(x) to x + c_i is an aligned vector store of the segment
@@ -58,16 +62,80 @@ __device__ __forceinline__ int src_row(int y, int cy, int ny, bool per, bool& wa
     return ys;
 }
 
+// The lane's place: V consecutive nodes x0.. of row y. w: lanes of a row segment (32, or the
+// power of two a row of fewer than 32 lanes is given, SEG only); sl: the lane's index in it;
+// rot: the segment holds one whole periodic row (nx = w V), so the x neighbours across the
+// row's ends are its last and first lanes (SEG only). Batches use the whole-warp form.
+struct Lane {
+    int x0, y, sl, w;
+    bool active, first, last, rot;
+};
+
+// SEG: blocks of several rows (rows of fewer than 128 lanes), shaped by block_for_rows; else
+// one row per block (1-D blocks, row = blockIdx.y, which keeps the row arithmetic uniform
+// across the warp: computed from threadIdx.y it measured 5-7 % slower at 4096^2).
+template <int STORE, bool SEG>
+__device__ __forceinline__ Lane lane_of(const StepParams& P) {
+    constexpr int V = VT<STORE>::V;
+    Lane l;
+    l.x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+    if constexpr (SEG) {
+        l.w = blockDim.x < 32 ? int(blockDim.x) : 32;
+        l.sl = threadIdx.x & (l.w - 1);
+        l.y = blockIdx.y * blockDim.y + threadIdx.y;
+        l.active = l.x0 < P.n[0] && l.y < P.n[1];
+        l.rot = P.per[0] && P.n[0] == l.w * V;
+    } else {
+        l.w = 32;
+        l.sl = threadIdx.x & 31;
+        l.y = blockIdx.y;
+        l.active = l.x0 < P.n[0];
+        l.rot = false;
+    }
+    l.first = l.sl == 0;
+    l.last = l.active && (l.sl == l.w - 1 || l.x0 + V >= P.n[0]);
+    return l;
+}
+
+// The value of lane sl - 1 / sl + 1: cyclically within the segment (SEG), else the plain warp
+// shuffle (the first / last lane's own value, which its halo replaces).
+template <bool SEG>
+__device__ __forceinline__ uint32_t from_prev(const Lane& l, uint32_t x) {
+    if constexpr (SEG) return __shfl_sync(kFull, x, (l.sl + l.w - 1) & (l.w - 1), l.w);
+    else return __shfl_up_sync(kFull, x, 1);
+}
+template <bool SEG>
+__device__ __forceinline__ uint32_t from_next(const Lane& l, uint32_t x) {
+    if constexpr (SEG) return __shfl_sync(kFull, x, (l.sl + 1) & (l.w - 1), l.w);
+    else return __shfl_down_sync(kFull, x, 1);
+}
+
+// Block shape (lanes along x, rows) for rows of nx nodes: whole warps for rows of 32 lanes or
+// more, power-of-two segments of a warp for shorter rows (the SEG kernels).
+inline dim3 block_for_rows(int nx, int V) {
+    const int need = (nx + V - 1) / V;
+    if (need < 32) {
+        int w = 1;
+        while (w < need) w <<= 1;
+        return dim3(w, kThreads / w);
+    }
+    int lanes = (need + 31) / 32 * 32;
+    if (lanes > kThreads) lanes = kThreads;
+    return dim3(lanes, kThreads / lanes);
+}
+
 // Load the pulled row segments of all 9 directions into v[] (raw storage elements), already
 // shifted along x. READ_OPP selects the AA-odd reading (source slot opp(i), bounce-back slot
 // i) instead of the two-buffer one (source slot i, bounce-back slot opp(i)).
-template <int STORE, bool READ_OPP, bool NC, bool EDGE>
+template <int STORE, bool READ_OPP, bool NC, bool EDGE, bool SEG = false>
 __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT<STORE>::E* A,
-                                          int x0, int y, bool active, bool first, bool last,
-                                          uint4 (&v)[9], float (&lid)[9]) {
+                                          const Lane& l, uint4 (&v)[9], float (&lid)[9]) {
     using E = typename VT<STORE>::E;
     constexpr int V = VT<STORE>::V;
     const int nx = P.n[0], ny = P.n[1], N = P.N;
+    const int x0 = l.x0, y = l.y;
+    const bool active = l.active;
+    const bool first = l.first && !l.rot, last = l.last && !l.rot;  // lanes that take a halo
     const bool perx = P.per[0], pery = P.per[1];
     uint32_t halo[9];
 #pragma unroll
@@ -107,11 +175,11 @@ __device__ __forceinline__ void pull_rows(const StepParams& P, const typename VT
         bool wall, top;
         src_row<EDGE>(y, L::cy(i), ny, pery, wall, top);
         if (cx == 1) {
-            uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
+            uint32_t up = from_prev<SEG>(l, elem<V>(v[i], V - 1));
             if (first) up = halo[i];
             if (!wall) v[i] = shift_up<V>(v[i], up);
         } else {
-            uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
+            uint32_t dn = from_next<SEG>(l, elem<V>(v[i], 0));
             if (last) dn = halo[i];
             if (!wall) v[i] = shift_down<V>(v[i], dn);
         }
@@ -183,35 +251,26 @@ __device__ __forceinline__ void collide_lane(const StepParams& P, uint4 (&v)[9],
     }
 }
 
-struct Lane {
-    int x0, y, lane;
-    bool active, first, last;
-};
-
-template <int STORE>
-__device__ __forceinline__ Lane lane_of(const StepParams& P) {
-    constexpr int V = VT<STORE>::V;
-    Lane l;
-    l.lane = threadIdx.x & 31;
-    l.x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
-    l.y = blockIdx.y;
-    l.active = l.x0 < P.n[0];
-    l.first = l.lane == 0;
-    l.last = l.active && (l.lane == 31 || l.x0 + V >= P.n[0]);
-    return l;
-}
-
 // A row next to a y wall (only those carry wall and lid logic).
 __device__ __forceinline__ bool edge_row(const StepParams& P, int y) {
     return !P.per[1] && (y == 0 || y == P.n[1] - 1);
 }
+// Whether the warp takes the wall path: any of its rows is next to a y wall (all 32 lanes
+// call this, before any of them can leave).
+template <bool SEG>
+__device__ __forceinline__ bool edge_warp(const StepParams& P, const Lane& l) {
+    const bool e = edge_row(P, l.y);
+    if constexpr (SEG) return l.w < 32 ? __any_sync(kFull, e) : e;
+    else return e;
+}
 
-template <int STORE, int COLL, bool FORCE, bool EDGE, bool PACK = (COLL != LBM_MRT)>
+template <int STORE, int COLL, bool FORCE, bool EDGE, bool PACK = (COLL != LBM_MRT),
+          bool SEG = false>
 __device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<STORE>::E* A,
                                        typename VT<STORE>::E* B, const Lane& l) {
     uint4 v[9];
     float lid[9];
-    pull_rows<STORE, false, true, EDGE>(P, A, l.x0, l.y, l.active, l.first, l.last, v, lid);
+    pull_rows<STORE, false, true, EDGE, SEG>(P, A, l, v, lid);
     if (!l.active) return;
     const float zero[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     collide_lane<STORE, COLL, FORCE, EDGE, PACK>(P, v, lid, zero);
@@ -220,15 +279,16 @@ __device__ __forceinline__ void ab_row(const StepParams& P, const typename VT<ST
     for (int i = 0; i < 9; ++i) st_cs(B + i * P.N + n0, v[i]);
 }
 
-template <int STORE, int COLL, bool FORCE>
+template <int STORE, int COLL, bool FORCE, bool SEG>
 __global__ void __launch_bounds__(kThreads)
 k_d2q9_ab(const StepParams P, const void* __restrict__ Av, void* __restrict__ Bv) {
     using E = typename VT<STORE>::E;
     const E* __restrict__ A = static_cast<const E*>(Av);
     E* __restrict__ B = static_cast<E*>(Bv);
-    const Lane l = lane_of<STORE>(P);
-    if (edge_row(P, l.y)) ab_row<STORE, COLL, FORCE, true>(P, A, B, l);
-    else ab_row<STORE, COLL, FORCE, false>(P, A, B, l);
+    constexpr bool pack = COLL != LBM_MRT;
+    const Lane l = lane_of<STORE, SEG>(P);
+    if (edge_warp<SEG>(P, l)) ab_row<STORE, COLL, FORCE, true, pack, SEG>(P, A, B, l);
+    else ab_row<STORE, COLL, FORCE, false, pack, SEG>(P, A, B, l);
 }
 
 template <int STORE, int COLL, bool FORCE>
@@ -248,7 +308,7 @@ k_d2q9_aa_even(const StepParams P, void* Av) {
     for (int i = 0; i < 9; ++i) st_cs(A + L::opp(i) * P.N + n0, v[i]);
 }
 
-template <int STORE, int COLL, bool FORCE, bool EDGE>
+template <int STORE, int COLL, bool FORCE, bool EDGE, bool SEG>
 __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STORE>::E* A,
                                            const Lane& l) {
     using E = typename VT<STORE>::E;
@@ -256,7 +316,7 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
     const int nx = P.n[0], ny = P.n[1], N = P.N;
     uint4 v[9];
     float lid[9];
-    pull_rows<STORE, true, false, EDGE>(P, A, l.x0, l.y, l.active, l.first, l.last, v, lid);
+    pull_rows<STORE, true, false, EDGE, SEG>(P, A, l, v, lid);
     // destinations x + c_i: whole-row wall bounces carry the lid term with the push sign
     float sub[9];
     bool dwall[9];
@@ -282,23 +342,23 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
         if (cx == 0) {
             if (l.active) st_plain(plane + l.x0, v[i]);
         } else if (cx == 1) {
-            const uint32_t up = __shfl_up_sync(kFull, elem<V>(v[i], V - 1), 1);
+            const uint32_t up = from_prev<SEG>(l, elem<V>(v[i], V - 1));
             if (!l.active) continue;
             const uint4 su = shift_up<V>(v[i], up);
-            if (!l.first) st_plain(plane + l.x0, su);
+            if (!l.first || l.rot) st_plain(plane + l.x0, su);
             else st_tail<V>(plane + l.x0, su);  // slot x0 belongs to the previous warp
-            if (l.last) {
+            if (l.last && !l.rot) {
                 E* dst = l.x0 + V < nx ? plane + l.x0 + V
                                        : (P.per[0] ? plane : bb + nx - 1);
                 st1(dst, elem<V>(v[i], V - 1));
             }
         } else {
-            const uint32_t dn = __shfl_down_sync(kFull, elem<V>(v[i], 0), 1);
+            const uint32_t dn = from_next<SEG>(l, elem<V>(v[i], 0));
             if (!l.active) continue;
             const uint4 sd = shift_down<V>(v[i], dn);
-            if (!l.last) st_plain(plane + l.x0, sd);
+            if (!l.last || l.rot) st_plain(plane + l.x0, sd);
             else st_head<V>(plane + l.x0, sd);  // slot x0 + V - 1 belongs to the next warp
-            if (l.first) {
+            if (l.first && !l.rot) {
                 E* dst = l.x0 > 0 ? plane + l.x0 - 1 : (P.per[0] ? plane + nx - 1 : bb);
                 st1(dst, elem<V>(v[i], 0));
             }
@@ -306,14 +366,14 @@ __device__ __forceinline__ void aa_odd_row(const StepParams& P, typename VT<STOR
     }
 }
 
-template <int STORE, int COLL, bool FORCE>
+template <int STORE, int COLL, bool FORCE, bool SEG>
 __global__ void __launch_bounds__(kThreads)
 k_d2q9_aa_odd(const StepParams P, void* Av) {
     using E = typename VT<STORE>::E;
     E* A = static_cast<E*>(Av);
-    const Lane l = lane_of<STORE>(P);
-    if (edge_row(P, l.y)) aa_odd_row<STORE, COLL, FORCE, true>(P, A, l);
-    else aa_odd_row<STORE, COLL, FORCE, false>(P, A, l);
+    const Lane l = lane_of<STORE, SEG>(P);
+    if (edge_warp<SEG>(P, l)) aa_odd_row<STORE, COLL, FORCE, true, SEG>(P, A, l);
+    else aa_odd_row<STORE, COLL, FORCE, false, SEG>(P, A, l);
 }
 
 template <int STORE, int COLL, bool FORCE>
@@ -331,11 +391,20 @@ int go(const StepParams& P, const void* src, void* dst, int pattern, cudaStream_
         return int(cudaGetLastError());
     }
     const int per_row = P.n[0] / V;
+    if (per_row < kThreads) {  // rows of fewer than 128 lanes: several rows per block
+        const dim3 block = block_for_rows(P.n[0], V);
+        const dim3 grid((per_row + block.x - 1) / block.x, (P.n[1] + block.y - 1) / block.y);
+        if (pattern == LBM_PATTERN_AB)
+            k_d2q9_ab<STORE, COLL, FORCE, true><<<grid, block, 0, s>>>(P, src, dst);
+        else
+            k_d2q9_aa_odd<STORE, COLL, FORCE, true><<<grid, block, 0, s>>>(P, dst);
+        return int(cudaGetLastError());
+    }
     const dim3 grid((per_row + kThreads - 1) / kThreads, P.n[1]);
     if (pattern == LBM_PATTERN_AB)
-        k_d2q9_ab<STORE, COLL, FORCE><<<grid, kThreads, 0, s>>>(P, src, dst);
+        k_d2q9_ab<STORE, COLL, FORCE, false><<<grid, kThreads, 0, s>>>(P, src, dst);
     else
-        k_d2q9_aa_odd<STORE, COLL, FORCE><<<grid, kThreads, 0, s>>>(P, dst);
+        k_d2q9_aa_odd<STORE, COLL, FORCE, false><<<grid, kThreads, 0, s>>>(P, dst);
     return int(cudaGetLastError());
 }
 
@@ -418,7 +487,9 @@ k_d2q9_batch_ab(const BatchLattice* __restrict__ item_tab, int items,
         const int vidx = local * 32 + lane;
         const int nvec = vrow * P.n[1];
         Lane l;
-        l.lane = lane;
+        l.sl = lane;
+        l.w = 32;
+        l.rot = false;
         l.active = vidx < nvec;
         // row of the lane's vector: from the item's first row, a few whole rows further
         int xv = __ldg(&bl.xv0) + lane, y = __ldg(&bl.y0);
