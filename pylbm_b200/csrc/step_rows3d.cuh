@@ -359,7 +359,8 @@ inline dim3 block_for_rows(int nx, int V, bool seg) {
 }
 
 // Whether a launch takes the segmented kernel: rows of fewer than 32 lanes, and every MRT or
-// forced launch (those are compute-bound and keep one instantiation).
+// forced launch (those keep one instantiation each, to bound the compile time: MRT is
+// compute-bound, and forced steps are not the throughput configurations).
 template <int COLL, bool FORCE>
 inline bool use_seg(int nx, int V) {
     return COLL == LBM_MRT || FORCE || (nx + V - 1) / V < 32;
