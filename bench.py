@@ -87,7 +87,8 @@ BATCHES = {
 # the configurations measured beside the default workload (``extra`` of the JSON line)
 EXTRA_SINGLE = ("d2q9-trt-ab-f32", "d2q9-bgk-aa-f32", "d2q9-trt-aa-f32", "d2q9-bgk-ab-f16",
                 "d2q9-bgk-ab-bf16", "d2q9-bgk-aa-f16", "d3q19-trt-ab-f32", "d3q19-trt-ab-f16",
-                "d3q19-trt-ab-bf16", "d3q19-trt-aa-f32", "d3q19-trt-aa-f16")
+                "d3q19-trt-ab-bf16", "d3q19-trt-aa-f32", "d3q19-trt-aa-f16", "d3q19-mrt-ab-f32",
+                "d3q19-mrt-ab-f16", "d3q19-mrt-aa-f16")
 EXTRA_WARMUP, EXTRA_STEPS = 3, 3
 HBM3E_SPEC_GBS = 8000.0  # B200 HBM3e specification (DGX figure)
 
